@@ -1,0 +1,166 @@
+/*
+ * luthe.h -- C ABI of the B200 KS+PBS engine.
+ *
+ * The engine is a drop-in for the HPU's PBS processing element (pe_pbs) and
+ * its linear-DOp neighbour (pe_alu).  On the HPU these are driven by DOps
+ * (docs/dop.md:82-165; binary form fw/ublaze/src/hpu_dop_fmt.h:43-140): a PBS
+ * DOp "PBS Dst Src LUT" reads a BLWE (k*N+1 u64) from the register file,
+ * key-switches it, blind-rotates a LUT GLWE selected by `gid`, sample-extracts
+ * the result and writes it back.  Here a batch of such DOps is one call; the
+ * register file is replaced by caller-owned device (or host) buffers.
+ *
+ * Conventions
+ *  - All pointers named d_* are device pointers, h_* host pointers.  The caller
+ *    owns every buffer passed in.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *  - Functions return LUTHE_OK or one of the LUTHE_E_* codes; the message of
+ *    the last failure on the calling thread is in luthe_last_error().  Errors
+ *    are reported, never hidden: there is no CPU fallback.
+ *  - A context is not thread-safe; one thread owns it (the HPU firmware loop
+ *    is single-threaded too: fw/ublaze/src/ucore_fw.c:68).
+ *
+ * Data formats (u64 torus values mod 2^64 unless stated)
+ *  - BLWE: N mask coefficients in natural order, then the body
+ *    (the order of the reference's input/output BLWE test vectors).
+ *  - KSK:  u32 words mod 2^ks_width, index (x*(k*N) + y)*ks_level + z, x in
+ *    [0, n] (the body column last), y the BLWE mask coefficient, z the level
+ *    (z = 0 is the least significant digit, weight 2^(ks_base_log*(z+1)))
+ *    -- the order of the reference's ksk_hwo files with one channel.
+ *  - BSK:  standard domain over Z_p, p = 2^64 - 2^32 + 1 (values < p), index
+ *    ((i*2 + row)*2 + col)*N + c: GGSW of LWE-key bit i, row = decomposed GLWE
+ *    component (0 mask, 1 body), col = output component.  The engine converts
+ *    it to its own evaluation layout on upload (the HPU too receives its BSK
+ *    pre-transformed from the host: hw/module/bsk/module/bsk_manager).
+ *  - LUT:  trivial GLWE, mask polynomial then body polynomial, natural order.
+ */
+#ifndef LUTHE_H
+#define LUTHE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LUTHE_OK 0
+#define LUTHE_E_PARAM 1   /* bad argument or unsupported parameter set */
+#define LUTHE_E_BUDGET 2  /* HBM admission budget exceeded */
+#define LUTHE_E_TIMEOUT 3 /* a bounded device wait ran out */
+#define LUTHE_E_CUDA 4    /* CUDA runtime error (no device, launch failure...) */
+#define LUTHE_E_STATE 5   /* keys or LUTs not uploaded yet */
+
+/* Crypto parameter set (hw/module/param/module/<set>/rtl/param_tfhe_definition_pkg.sv). */
+typedef struct luthe_params {
+    uint32_t lwe_dim;      /* n      (804) */
+    uint32_t glwe_dim;     /* k      (1)   */
+    uint32_t poly_size;    /* N      (2048) */
+    uint32_t pbs_base_log; /* 23 */
+    uint32_t pbs_level;    /* 1  */
+    uint32_t ks_base_log;  /* 3  */
+    uint32_t ks_level;     /* 6  */
+    uint32_t ks_width;     /* 21: KS modulus 2^21 (MOD_KSK_W) */
+    uint32_t msg_width;    /* 2  */
+    uint32_t carry_width;  /* 2  */
+} luthe_params;
+
+typedef struct luthe_ctx luthe_ctx;
+
+/* Linear DOps (docs/dop.md:82-100; pea_alu_core.sv:59-61,124-161). */
+enum luthe_lwe_op {
+    LUTHE_OP_ADD = 0,  /* dst = a + b            */
+    LUTHE_OP_SUB = 1,  /* dst = a - b            */
+    LUTHE_OP_MAC = 2,  /* dst = a * imm + b      */
+    LUTHE_OP_ADDS = 3, /* dst = a + imm*Delta    */
+    LUTHE_OP_SUBS = 4, /* dst = a - imm*Delta    */
+    LUTHE_OP_SSUB = 5, /* dst = imm*Delta - a    */
+    LUTHE_OP_MULS = 6  /* dst = a * imm          */
+};
+
+/* Fill `p` with the engine's parameter set (n=804, k=1, N=2048, PBS 23x1,
+ * KS 3x6 mod 2^21, 2-bit message + 2-bit carry). */
+void luthe_params_default(luthe_params *p);
+
+const char *luthe_last_error(void);
+
+/* Context: binds a CUDA device; `hbm_budget` caps the device bytes the context
+ * may hold (0 = 80 GB).  Replaces the HPU bring-up the host backend performs
+ * over PCIe (docs/hpu.md:42-54). */
+int luthe_ctx_create(const luthe_params *p, int device, uint64_t hbm_budget, luthe_ctx **out);
+void luthe_ctx_destroy(luthe_ctx *ctx);
+uint64_t luthe_device_bytes(const luthe_ctx *ctx);
+
+/* Key material (bsk_manager.sv / ksk_manager.sv: keys resident before BR). */
+int luthe_upload_bsk(luthe_ctx *ctx, const uint64_t *h_bsk_std_p);
+int luthe_upload_ksk(luthe_ctx *ctx, const uint32_t *h_ksk);
+/* LUT memory, indexed by the PBS DOp's gid (dflt_cfg.toml:18-19 lut_mem). */
+int luthe_upload_luts(luthe_ctx *ctx, const uint64_t *h_glwe, uint32_t count);
+
+/* Pre-size the per-call scratch for batches up to `max_count` ciphertexts, so
+ * later calls (and graph captures) allocate nothing. */
+int luthe_reserve(luthe_ctx *ctx, size_t max_count);
+
+/* Batched PBS DOp: KS + blind rotation + sample extract of `count` BLWEs with
+ * per-ciphertext LUT ids (PBS Dst Src LUT, docs/dop.md:101-111).  Replaces one
+ * pe_pbs batch (pe_pbs.sv:346-762) -- here every batch size in one launch. */
+int luthe_ks_pbs(luthe_ctx *ctx, const uint64_t *d_in, const uint32_t *d_lut_id, uint64_t *d_out, size_t count,
+                 void *stream);
+/* Same through host buffers (copies in, computes, copies out, synchronises).
+ * Pinned host memory gives the full PCIe/C2C bandwidth. */
+int luthe_ks_pbs_host(luthe_ctx *ctx, const uint64_t *h_in, const uint32_t *h_lut_id, uint64_t *h_out,
+                      size_t count);
+/* CUDA-graph form of luthe_ks_pbs: the first call for a given (pointers,
+ * count, stream) captures the launches, later calls replay the graph. */
+int luthe_ks_pbs_graph(luthe_ctx *ctx, const uint64_t *d_in, const uint32_t *d_lut_id, uint64_t *d_out,
+                       size_t count, void *stream);
+
+/* Stages on their own (pep_key_switch; pe_pbs BR + SXT). */
+int luthe_keyswitch(luthe_ctx *ctx, const uint64_t *d_in, uint32_t *d_out21, uint32_t *d_out2N, size_t count,
+                    void *stream);
+int luthe_blind_rotate(luthe_ctx *ctx, const uint32_t *d_lwe2N, const uint32_t *d_lut_id, uint64_t *d_out,
+                       size_t count, void *stream);
+
+/* Negacyclic NTT over Goldilocks, N = 2048 (ntt_core_gf64).  Forward output
+ * index k holds A(psi^(2k+1)), psi = 0x984ec5194d005735 (psi^64 = 8); the
+ * inverse includes 1/N.  luthe_ntt_mul computes INTT(NTT(a) * NTT(b)). */
+int luthe_ntt_fwd(luthe_ctx *ctx, const uint64_t *d_in, uint64_t *d_out, size_t count, void *stream);
+int luthe_ntt_inv(luthe_ctx *ctx, const uint64_t *d_in, uint64_t *d_out, size_t count, void *stream);
+int luthe_ntt_mul(luthe_ctx *ctx, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, size_t count,
+                  void *stream);
+
+/* Linear DOps on `count` BLWEs (pe_alu). */
+int luthe_lwe_op(luthe_ctx *ctx, int op, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, uint64_t imm,
+                 size_t count, void *stream);
+
+/* Blind-rotation launch shape: ciphertexts per CTA sharing one BSK slab (1 or
+ * 2) and CTAs per SM of the persistent grid.  luthe_autotune times the
+ * candidates on `sample` ciphertexts and keeps the fastest; it writes a JSON
+ * record of the trial into `json` (may be NULL). */
+int luthe_set_br_config(luthe_ctx *ctx, int cts_per_cta, int ctas_per_sm);
+int luthe_autotune(luthe_ctx *ctx, size_t sample, char *json, size_t json_cap);
+
+/* Device-side error flag of the last blind rotation (bounded waits). */
+int luthe_check_device_error(luthe_ctx *ctx);
+
+/* ------------------------------------------------------------ host helpers */
+
+/* Seeded key generation (binary keys, Gaussian noise: LWE sigma 2^-17.5,
+ * GLWE sigma 2^-51, relative to the modulus).  Buffers:
+ *   lwe_key[n], glwe_key[k*N], ksk[(n+1)*k*N*ks_level], bsk[n*4*N]. */
+int luthe_keygen(const luthe_params *p, uint64_t seed, uint32_t *lwe_key, uint32_t *glwe_key, uint32_t *ksk,
+                 uint64_t *bsk_std_p);
+/* Encrypt `count` messages (message+carry bits, < 2^(msg+carry)) under the
+ * GLWE key seen as an LWE key of dimension k*N. */
+int luthe_encrypt(const luthe_params *p, const uint32_t *glwe_key, const uint32_t *msgs, size_t count,
+                  uint64_t seed, uint64_t *blwe);
+/* Decrypt `count` BLWEs: msgs[i] = round(phase / Delta) mod 2^(1+msg+carry). */
+int luthe_decrypt(const luthe_params *p, const uint32_t *glwe_key, const uint64_t *blwe, size_t count,
+                  uint32_t *msgs);
+/* Build the trivial LUT GLWE for f given as table[2^(msg+carry)] (values
+ * < 2^(msg+carry)); the box layout of the reference's LUT test vectors. */
+int luthe_lut_build(const luthe_params *p, const uint32_t *table, uint64_t *glwe);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LUTHE_H */

@@ -1,0 +1,262 @@
+"""LUTHE-B200: a B200 (sm_100a) KS+PBS engine with the HPU's DOp surface.
+
+This module loads the in-tree engine library (``libluthe.so``) through ctypes
+and mirrors the reference's PBS/ALU operator interface:
+
+* :class:`Engine` -- one device context with resident keys and LUTs; its
+  methods are the batched DOps (``ks_pbs`` is ``PBS Dst Src LUT`` over a batch,
+  ``lwe_op`` the linear DOps of pe_alu, plus the KS/BR/NTT stages on their own).
+* :func:`keygen`, :func:`encrypt`, :func:`decrypt`, :func:`lut_build` -- host
+  helpers for seeded key material and test data.
+
+There is no fallback path: if the library is missing or the device cannot be
+used, calls raise :class:`LutheError`.
+"""
+import ctypes
+import json
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libluthe.so")
+
+OK, E_PARAM, E_BUDGET, E_TIMEOUT, E_CUDA, E_STATE = range(6)
+OP_ADD, OP_SUB, OP_MAC, OP_ADDS, OP_SUBS, OP_SSUB, OP_MULS = range(7)
+
+# exported symbols of include/luthe.h
+SYMBOLS = [
+    "luthe_params_default", "luthe_last_error", "luthe_ctx_create", "luthe_ctx_destroy", "luthe_device_bytes",
+    "luthe_upload_bsk", "luthe_upload_ksk", "luthe_upload_luts", "luthe_reserve", "luthe_ks_pbs",
+    "luthe_ks_pbs_host", "luthe_ks_pbs_graph", "luthe_keyswitch", "luthe_blind_rotate", "luthe_ntt_fwd",
+    "luthe_ntt_inv", "luthe_ntt_mul", "luthe_lwe_op", "luthe_set_br_config", "luthe_autotune",
+    "luthe_check_device_error", "luthe_keygen", "luthe_encrypt", "luthe_decrypt", "luthe_lut_build",
+]
+
+
+class LutheError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"luthe error {code}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint32) for name in (
+        "lwe_dim", "glwe_dim", "poly_size", "pbs_base_log", "pbs_level", "ks_base_log", "ks_level",
+        "ks_width", "msg_width", "carry_width")]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """The loaded engine library (built on first use if the sources are newer)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build
+            build.build_engine()
+        if not os.path.exists(LIB_PATH):
+            raise LutheError(E_CUDA, f"engine library missing: {LIB_PATH}")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, sz, u64, u32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint32
+        P = ctypes.POINTER(Params)
+        L.luthe_last_error.restype = ctypes.c_char_p
+        L.luthe_params_default.argtypes = [P]
+        L.luthe_ctx_create.argtypes = [P, ctypes.c_int, u64, ctypes.POINTER(vp)]
+        L.luthe_ctx_destroy.argtypes = [vp]
+        L.luthe_device_bytes.argtypes = [vp]
+        L.luthe_device_bytes.restype = u64
+        L.luthe_upload_bsk.argtypes = [vp, vp]
+        L.luthe_upload_ksk.argtypes = [vp, vp]
+        L.luthe_upload_luts.argtypes = [vp, vp, u32]
+        L.luthe_reserve.argtypes = [vp, sz]
+        for f in ("luthe_ks_pbs", "luthe_ks_pbs_graph"):
+            getattr(L, f).argtypes = [vp, vp, vp, vp, sz, vp]
+        L.luthe_ks_pbs_host.argtypes = [vp, vp, vp, vp, sz]
+        L.luthe_keyswitch.argtypes = [vp, vp, vp, vp, sz, vp]
+        L.luthe_blind_rotate.argtypes = [vp, vp, vp, vp, sz, vp]
+        L.luthe_ntt_fwd.argtypes = [vp, vp, vp, sz, vp]
+        L.luthe_ntt_inv.argtypes = [vp, vp, vp, sz, vp]
+        L.luthe_ntt_mul.argtypes = [vp, vp, vp, vp, sz, vp]
+        L.luthe_lwe_op.argtypes = [vp, ctypes.c_int, vp, vp, vp, u64, sz, vp]
+        L.luthe_set_br_config.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.luthe_autotune.argtypes = [vp, sz, ctypes.c_char_p, sz]
+        L.luthe_check_device_error.argtypes = [vp]
+        L.luthe_keygen.argtypes = [P, u64, vp, vp, vp, vp]
+        L.luthe_encrypt.argtypes = [P, vp, vp, sz, u64, vp]
+        L.luthe_decrypt.argtypes = [P, vp, vp, sz, vp]
+        L.luthe_lut_build.argtypes = [P, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _check(code):
+    if code != OK:
+        raise LutheError(code, lib().luthe_last_error().decode())
+
+
+def default_params(**over):
+    p = Params()
+    lib().luthe_params_default(ctypes.byref(p))
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags.c_contiguous
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        assert a.is_contiguous()
+        return a.data_ptr()
+    return int(a)
+
+
+# ------------------------------------------------------------- host helpers
+
+def keygen(params, seed):
+    """Seeded keys: lwe_key[n], glwe_key[N], ksk[(n+1)*N*L] (u32), bsk[n*4*N] over Z_p."""
+    n, N, L = params.lwe_dim, params.poly_size * params.glwe_dim, params.ks_level
+    k = {
+        "lwe_key": np.zeros(n, np.uint32),
+        "glwe_key": np.zeros(N, np.uint32),
+        "ksk": np.zeros((n + 1) * N * L, np.uint32),
+        "bsk": np.zeros(n * 4 * params.poly_size, np.uint64),
+    }
+    _check(lib().luthe_keygen(ctypes.byref(params), seed, _ptr(k["lwe_key"]), _ptr(k["glwe_key"]),
+                              _ptr(k["ksk"]), _ptr(k["bsk"])))
+    return k
+
+
+def encrypt(params, glwe_key, msgs, seed):
+    msgs = np.ascontiguousarray(msgs, np.uint32)
+    out = np.zeros((len(msgs), params.poly_size + 1), np.uint64)
+    _check(lib().luthe_encrypt(ctypes.byref(params), _ptr(glwe_key), _ptr(msgs), len(msgs), seed, _ptr(out)))
+    return out
+
+
+def decrypt(params, glwe_key, blwe):
+    blwe = np.ascontiguousarray(blwe, np.uint64).reshape(-1, params.poly_size + 1)
+    out = np.zeros(blwe.shape[0], np.uint32)
+    _check(lib().luthe_decrypt(ctypes.byref(params), _ptr(glwe_key), _ptr(blwe), blwe.shape[0], _ptr(out)))
+    return out
+
+
+def lut_build(params, table):
+    table = np.ascontiguousarray(table, np.uint32)
+    out = np.zeros(2 * params.poly_size, np.uint64)
+    _check(lib().luthe_lut_build(ctypes.byref(params), _ptr(table), _ptr(out)))
+    return out
+
+
+# ------------------------------------------------------------------- engine
+
+class Engine:
+    """A device context holding the BSK, KSK and LUT memory of the HPU's pe_pbs.
+
+    Device-pointer methods take torch CUDA tensors (or raw addresses) and a
+    stream (torch stream, raw handle, or None for the default stream).
+    """
+
+    def __init__(self, params=None, device=0, hbm_budget=0):
+        self.params = params or default_params()
+        self._h = None
+        h = ctypes.c_void_p()
+        _check(lib().luthe_ctx_create(ctypes.byref(self.params), device, hbm_budget, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().luthe_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @staticmethod
+    def _s(stream):
+        if stream is None:
+            return None
+        return getattr(stream, "cuda_stream", stream)
+
+    @property
+    def device_bytes(self):
+        return lib().luthe_device_bytes(self._h)
+
+    def upload_keys(self, keys):
+        self.upload_bsk(keys["bsk"])
+        self.upload_ksk(keys["ksk"])
+
+    def upload_bsk(self, bsk):
+        bsk = np.ascontiguousarray(bsk, np.uint64)
+        _check(lib().luthe_upload_bsk(self._h, _ptr(bsk)))
+
+    def upload_ksk(self, ksk):
+        ksk = np.ascontiguousarray(ksk, np.uint32)
+        _check(lib().luthe_upload_ksk(self._h, _ptr(ksk)))
+
+    def upload_luts(self, luts):
+        luts = np.ascontiguousarray(luts, np.uint64).reshape(-1, 2 * self.params.poly_size)
+        _check(lib().luthe_upload_luts(self._h, _ptr(luts), luts.shape[0]))
+
+    def reserve(self, count):
+        _check(lib().luthe_reserve(self._h, count))
+
+    def ks_pbs(self, d_in, d_ids, d_out, count, stream=None):
+        _check(lib().luthe_ks_pbs(self._h, _ptr(d_in), _ptr(d_ids), _ptr(d_out), count, self._s(stream)))
+
+    def ks_pbs_graph(self, d_in, d_ids, d_out, count, stream):
+        _check(lib().luthe_ks_pbs_graph(self._h, _ptr(d_in), _ptr(d_ids), _ptr(d_out), count, self._s(stream)))
+
+    def ks_pbs_host(self, blwe_in, lut_ids, out=None):
+        blwe_in = np.ascontiguousarray(blwe_in, np.uint64).reshape(-1, self.params.poly_size + 1)
+        lut_ids = np.ascontiguousarray(lut_ids, np.uint32)
+        if out is None:
+            out = np.empty_like(blwe_in)
+        _check(lib().luthe_ks_pbs_host(self._h, _ptr(blwe_in), _ptr(lut_ids), _ptr(out), blwe_in.shape[0]))
+        return out
+
+    def keyswitch(self, d_in, d_out21, d_out2N, count, stream=None):
+        _check(lib().luthe_keyswitch(self._h, _ptr(d_in), _ptr(d_out21), _ptr(d_out2N), count, self._s(stream)))
+
+    def blind_rotate(self, d_lwe2N, d_ids, d_out, count, stream=None):
+        _check(lib().luthe_blind_rotate(self._h, _ptr(d_lwe2N), _ptr(d_ids), _ptr(d_out), count, self._s(stream)))
+
+    def ntt_fwd(self, d_in, d_out, count, stream=None):
+        _check(lib().luthe_ntt_fwd(self._h, _ptr(d_in), _ptr(d_out), count, self._s(stream)))
+
+    def ntt_inv(self, d_in, d_out, count, stream=None):
+        _check(lib().luthe_ntt_inv(self._h, _ptr(d_in), _ptr(d_out), count, self._s(stream)))
+
+    def ntt_mul(self, d_a, d_b, d_out, count, stream=None):
+        _check(lib().luthe_ntt_mul(self._h, _ptr(d_a), _ptr(d_b), _ptr(d_out), count, self._s(stream)))
+
+    def lwe_op(self, op, d_a, d_b, d_out, imm, count, stream=None):
+        _check(lib().luthe_lwe_op(self._h, op, _ptr(d_a), _ptr(d_b), _ptr(d_out), imm, count, self._s(stream)))
+
+    def set_br_config(self, cts_per_cta, ctas_per_sm=1):
+        _check(lib().luthe_set_br_config(self._h, cts_per_cta, ctas_per_sm))
+
+    def autotune(self, sample=0):
+        buf = ctypes.create_string_buffer(4096)
+        _check(lib().luthe_autotune(self._h, sample, buf, 4096))
+        return json.loads(buf.value.decode())
+
+    def check_device_error(self):
+        _check(lib().luthe_check_device_error(self._h))

@@ -1,0 +1,517 @@
+// C ABI of the engine: context, key upload, batched KS+PBS, NTT, linear DOps,
+// CUDA-graph replay and the blind-rotation autotuner.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdarg.h>
+#include <string>
+#include <vector>
+#include "../../include/luthe.h"
+#include "kernels.cuh"
+
+using namespace luthe;
+
+static thread_local char g_err[512] = "";
+
+static int fail(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+    return code;
+}
+#define CUDA_TRY(expr)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (expr);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(LUTHE_E_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_),    \
+                        __FILE__, __LINE__);                                              \
+    } while (0)
+
+struct GraphEntry {
+    const void *in, *ids;
+    void *out;
+    size_t count;
+    cudaStream_t stream;
+    cudaGraphExec_t exec;
+};
+
+struct luthe_ctx {
+    luthe_params p;
+    int device = 0;
+    int nsm = 148;
+    uint64_t budget = 0, used = 0;
+    uint64_t *d_tw = nullptr;     // [2][8][256]
+    uint64_t *d_bsk = nullptr;    // [n][8][2][2][256]
+    uint32_t *d_ksk = nullptr;    // [kN*L][xpad]
+    uint32_t xpad = 0;
+    uint64_t *d_luts = nullptr;   // [nlut][2][N]
+    uint32_t nlut = 0;
+    uint32_t *d_err = nullptr;
+    // scratch
+    uint32_t *d_lwe2N = nullptr;  // [cap][n+1]
+    size_t cap = 0;
+    // host-path staging
+    uint64_t *d_hin = nullptr, *d_hout = nullptr;
+    uint32_t *d_hids = nullptr;
+    size_t hcap = 0;
+    BrConfig br{2, 1};
+    std::vector<GraphEntry> graphs;
+};
+
+extern "C" const char *luthe_last_error(void) { return g_err; }
+
+extern "C" void luthe_params_default(luthe_params *p)
+{
+    p->lwe_dim = 804;
+    p->glwe_dim = 1;
+    p->poly_size = 2048;
+    p->pbs_base_log = 23;
+    p->pbs_level = 1;
+    p->ks_base_log = 3;
+    p->ks_level = 6;
+    p->ks_width = 21;
+    p->msg_width = 2;
+    p->carry_width = 2;
+}
+
+static int check_params(const luthe_params *p)
+{
+    if (!p) return fail(LUTHE_E_PARAM, "null params");
+    if (p->glwe_dim != 1 || p->poly_size != (uint32_t)N || p->pbs_base_log != 23 || p->pbs_level != 1 ||
+        p->ks_base_log != (uint32_t)KS_BL || p->ks_level != (uint32_t)KS_L || p->ks_width != (uint32_t)KS_W)
+        return fail(LUTHE_E_PARAM,
+                    "unsupported parameter set (engine is built for k=1 N=2048 PBS 23x1 KS 3x6 mod 2^21)");
+    if (p->lwe_dim == 0 || p->lwe_dim > 4096) return fail(LUTHE_E_PARAM, "lwe_dim %u out of range", p->lwe_dim);
+    if (p->msg_width + p->carry_width + 1 > 32) return fail(LUTHE_E_PARAM, "message width too large");
+    return LUTHE_OK;
+}
+
+static int dalloc(luthe_ctx *c, void **ptr, size_t bytes)
+{
+    if (c->used + bytes > c->budget)
+        return fail(LUTHE_E_BUDGET, "HBM budget exceeded: %llu + %zu > %llu bytes", (unsigned long long)c->used,
+                    bytes, (unsigned long long)c->budget);
+    CUDA_TRY(cudaMalloc(ptr, bytes));
+    c->used += bytes;
+    return LUTHE_OK;
+}
+static void dfree(luthe_ctx *c, void *ptr, size_t bytes)
+{
+    if (ptr) {
+        cudaFree(ptr);
+        c->used -= bytes;
+    }
+}
+
+static void drop_graphs(luthe_ctx *c)
+{
+    for (auto &g : c->graphs) cudaGraphExecDestroy(g.exec);
+    c->graphs.clear();
+}
+
+extern "C" int luthe_ctx_create(const luthe_params *p, int device, uint64_t budget, luthe_ctx **out)
+{
+    if (!out) return fail(LUTHE_E_PARAM, "null out");
+    *out = nullptr;
+    int r = check_params(p);
+    if (r) return r;
+    CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(LUTHE_E_CUDA, "device %d is sm_%d%d; this build targets sm_100a", device,
+                                      prop.major, prop.minor);
+    luthe_ctx *c = new luthe_ctx();
+    c->p = *p;
+    c->device = device;
+    c->nsm = prop.multiProcessorCount;
+    c->budget = budget ? budget : 80ull * 1000 * 1000 * 1000;
+    std::vector<uint64_t> tw(4096);
+    build_twiddles(tw.data());
+    if ((r = dalloc(c, (void **)&c->d_tw, 4096 * 8)) || (r = dalloc(c, (void **)&c->d_err, 4))) {
+        luthe_ctx_destroy(c);
+        return r;
+    }
+    cudaError_t e = cudaMemcpy(c->d_tw, tw.data(), 4096 * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, 4);
+    if (e == cudaSuccess) e = br_set_attributes(BrConfig{1, 1}, p->lwe_dim);
+    if (e == cudaSuccess) e = br_set_attributes(BrConfig{2, 1}, p->lwe_dim);
+    if (e != cudaSuccess) {
+        luthe_ctx_destroy(c);
+        return fail(LUTHE_E_CUDA, "context init: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return LUTHE_OK;
+}
+
+extern "C" void luthe_ctx_destroy(luthe_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    drop_graphs(c);
+    const size_t n = c->p.lwe_dim;
+    dfree(c, c->d_tw, 4096 * 8);
+    dfree(c, c->d_err, 4);
+    dfree(c, c->d_bsk, n * SLAB_BYTES);
+    dfree(c, c->d_ksk, (size_t)N * KS_L * c->xpad * 4);
+    dfree(c, c->d_luts, (size_t)c->nlut * 2 * N * 8);
+    dfree(c, c->d_lwe2N, c->cap * (n + 1) * 4);
+    dfree(c, c->d_hin, c->hcap * (N + 1) * 8);
+    dfree(c, c->d_hout, c->hcap * (N + 1) * 8);
+    dfree(c, c->d_hids, c->hcap * 4);
+    delete c;
+}
+
+extern "C" uint64_t luthe_device_bytes(const luthe_ctx *c) { return c ? c->used : 0; }
+
+extern "C" int luthe_upload_bsk(luthe_ctx *c, const uint64_t *h)
+{
+    if (!c || !h) return fail(LUTHE_E_PARAM, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t n = c->p.lwe_dim, words = n * 4 * N;
+    for (size_t i = 0; i < words; i++)
+        if (h[i] >= 0xFFFFFFFF00000001ull) return fail(LUTHE_E_PARAM, "BSK word %zu is not reduced mod p", i);
+    int r;
+    if (!c->d_bsk && (r = dalloc(c, (void **)&c->d_bsk, n * SLAB_BYTES))) return r;
+    uint64_t *d_std = nullptr;
+    if ((r = dalloc(c, (void **)&d_std, words * 8))) return r;
+    cudaError_t e = cudaMemcpy(d_std, h, words * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_bsk_prepare(d_std, c->d_bsk, c->d_tw, (uint32_t)n, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    dfree(c, d_std, words * 8);
+    if (e != cudaSuccess) return fail(LUTHE_E_CUDA, "BSK upload: %s", cudaGetErrorString(e));
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_upload_ksk(luthe_ctx *c, const uint32_t *h)
+{
+    if (!c || !h) return fail(LUTHE_E_PARAM, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t n = c->p.lwe_dim, K = (size_t)N * KS_L;
+    const uint32_t xpad = (uint32_t)(((n + 1) + KS_BN - 1) / KS_BN * KS_BN);
+    std::vector<uint32_t> t((size_t)K * xpad, 0);
+    const uint32_t M = (1u << KS_W) - 1;
+    for (size_t x = 0; x <= n; x++)
+        for (size_t k = 0; k < K; k++) t[k * xpad + x] = h[x * K + k] & M;
+    int r;
+    if (!c->d_ksk) {
+        if ((r = dalloc(c, (void **)&c->d_ksk, K * xpad * 4))) return r;
+        c->xpad = xpad;
+    }
+    CUDA_TRY(cudaMemcpy(c->d_ksk, t.data(), K * xpad * 4, cudaMemcpyHostToDevice));
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_upload_luts(luthe_ctx *c, const uint64_t *h, uint32_t count)
+{
+    if (!c || !h || count == 0) return fail(LUTHE_E_PARAM, "bad LUT arguments");
+    CUDA_TRY(cudaSetDevice(c->device));
+    drop_graphs(c);
+    dfree(c, c->d_luts, (size_t)c->nlut * 2 * N * 8);
+    c->d_luts = nullptr;
+    c->nlut = 0;
+    int r;
+    if ((r = dalloc(c, (void **)&c->d_luts, (size_t)count * 2 * N * 8))) return r;
+    c->nlut = count;
+    CUDA_TRY(cudaMemcpy(c->d_luts, h, (size_t)count * 2 * N * 8, cudaMemcpyHostToDevice));
+    return LUTHE_OK;
+}
+
+static int ensure_scratch(luthe_ctx *c, size_t count)
+{
+    if (count <= c->cap) return LUTHE_OK;
+    drop_graphs(c);
+    const size_t n1 = c->p.lwe_dim + 1;
+    dfree(c, c->d_lwe2N, c->cap * n1 * 4);
+    c->d_lwe2N = nullptr;
+    c->cap = 0;
+    int r = dalloc(c, (void **)&c->d_lwe2N, count * n1 * 4);
+    if (r) return r;
+    c->cap = count;
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_reserve(luthe_ctx *c, size_t max_count)
+{
+    if (!c) return fail(LUTHE_E_PARAM, "null ctx");
+    CUDA_TRY(cudaSetDevice(c->device));
+    return ensure_scratch(c, max_count);
+}
+
+static int need_keys(luthe_ctx *c)
+{
+    if (!c) return fail(LUTHE_E_PARAM, "null ctx");
+    if (!c->d_bsk || !c->d_ksk) return fail(LUTHE_E_STATE, "keys not uploaded");
+    if (!c->d_luts) return fail(LUTHE_E_STATE, "LUTs not uploaded");
+    return LUTHE_OK;
+}
+
+static int enqueue_ks_pbs(luthe_ctx *c, const uint64_t *d_in, const uint32_t *d_ids, uint64_t *d_out, size_t count,
+                          cudaStream_t s)
+{
+    const uint32_t n = c->p.lwe_dim;
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s));
+    CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out,
+                                 count, n, c->d_err, s));
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_ks_pbs(luthe_ctx *c, const uint64_t *d_in, const uint32_t *d_ids, uint64_t *d_out,
+                            size_t count, void *stream)
+{
+    int r = need_keys(c);
+    if (r) return r;
+    if (count == 0) return LUTHE_OK;
+    if (!d_in || !d_ids || !d_out) return fail(LUTHE_E_PARAM, "null buffer");
+    CUDA_TRY(cudaSetDevice(c->device));
+    if ((r = ensure_scratch(c, count))) return r;
+    return enqueue_ks_pbs(c, d_in, d_ids, d_out, count, (cudaStream_t)stream);
+}
+
+extern "C" int luthe_ks_pbs_graph(luthe_ctx *c, const uint64_t *d_in, const uint32_t *d_ids, uint64_t *d_out,
+                                  size_t count, void *stream)
+{
+    int r = need_keys(c);
+    if (r) return r;
+    if (count == 0) return LUTHE_OK;
+    if (!d_in || !d_ids || !d_out) return fail(LUTHE_E_PARAM, "null buffer");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!s) return fail(LUTHE_E_PARAM, "graph capture needs a non-default stream");
+    if ((r = ensure_scratch(c, count))) return r;
+    for (auto &g : c->graphs)
+        if (g.in == d_in && g.ids == d_ids && g.out == d_out && g.count == count && g.stream == s) {
+            CUDA_TRY(cudaGraphLaunch(g.exec, s));
+            return LUTHE_OK;
+        }
+    cudaGraph_t graph;
+    CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    r = enqueue_ks_pbs(c, d_in, d_ids, d_out, count, s);
+    cudaError_t e = cudaStreamEndCapture(s, &graph);
+    if (r) return r;
+    if (e != cudaSuccess) return fail(LUTHE_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(LUTHE_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    if (c->graphs.size() >= 8) {
+        cudaGraphExecDestroy(c->graphs.front().exec);
+        c->graphs.erase(c->graphs.begin());
+    }
+    c->graphs.push_back(GraphEntry{d_in, d_ids, d_out, count, s, exec});
+    CUDA_TRY(cudaGraphLaunch(exec, s));
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_ks_pbs_host(luthe_ctx *c, const uint64_t *h_in, const uint32_t *h_ids, uint64_t *h_out,
+                                 size_t count)
+{
+    int r = need_keys(c);
+    if (r) return r;
+    if (count == 0) return LUTHE_OK;
+    if (!h_in || !h_ids || !h_out) return fail(LUTHE_E_PARAM, "null buffer");
+    CUDA_TRY(cudaSetDevice(c->device));
+    for (size_t i = 0; i < count; i++)
+        if (h_ids[i] >= c->nlut) return fail(LUTHE_E_PARAM, "LUT id %u at %zu out of range", h_ids[i], i);
+    if (count > c->hcap) {
+        drop_graphs(c);
+        dfree(c, c->d_hin, c->hcap * (N + 1) * 8);
+        dfree(c, c->d_hout, c->hcap * (N + 1) * 8);
+        dfree(c, c->d_hids, c->hcap * 4);
+        c->d_hin = c->d_hout = nullptr;
+        c->d_hids = nullptr;
+        c->hcap = 0;
+        if ((r = dalloc(c, (void **)&c->d_hin, count * (N + 1) * 8)) ||
+            (r = dalloc(c, (void **)&c->d_hout, count * (N + 1) * 8)) ||
+            (r = dalloc(c, (void **)&c->d_hids, count * 4)))
+            return r;
+        c->hcap = count;
+    }
+    if ((r = ensure_scratch(c, count))) return r;
+    cudaStream_t s = 0;
+    CUDA_TRY(cudaMemcpyAsync(c->d_hin, h_in, count * (N + 1) * 8, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(c->d_hids, h_ids, count * 4, cudaMemcpyHostToDevice, s));
+    if ((r = enqueue_ks_pbs(c, c->d_hin, c->d_hids, c->d_hout, count, s))) return r;
+    CUDA_TRY(cudaMemcpyAsync(h_out, c->d_hout, count * (N + 1) * 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return luthe_check_device_error(c);
+}
+
+extern "C" int luthe_keyswitch(luthe_ctx *c, const uint64_t *d_in, uint32_t *d_out21, uint32_t *d_out2N,
+                               size_t count, void *stream)
+{
+    if (!c) return fail(LUTHE_E_PARAM, "null ctx");
+    if (!c->d_ksk) return fail(LUTHE_E_STATE, "KSK not uploaded");
+    if (count == 0) return LUTHE_OK;
+    if (!d_in || !d_out2N) return fail(LUTHE_E_PARAM, "null buffer");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, d_out21, d_out2N, count, c->p.lwe_dim, c->xpad,
+                              (cudaStream_t)stream));
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_blind_rotate(luthe_ctx *c, const uint32_t *d_lwe2N, const uint32_t *d_ids, uint64_t *d_out,
+                                  size_t count, void *stream)
+{
+    int r = need_keys(c);
+    if (r) return r;
+    if (count == 0) return LUTHE_OK;
+    if (!d_lwe2N || !d_ids || !d_out) return fail(LUTHE_E_PARAM, "null buffer");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(launch_blind_rotate(c->br, c->nsm, d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out, count,
+                                 c->p.lwe_dim, c->d_err, (cudaStream_t)stream));
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_ntt_fwd(luthe_ctx *c, const uint64_t *d_in, uint64_t *d_out, size_t count, void *stream)
+{
+    if (!c || (count && (!d_in || !d_out))) return fail(LUTHE_E_PARAM, "bad argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(launch_ntt_fwd(d_in, d_out, c->d_tw, count, (cudaStream_t)stream));
+    return LUTHE_OK;
+}
+extern "C" int luthe_ntt_inv(luthe_ctx *c, const uint64_t *d_in, uint64_t *d_out, size_t count, void *stream)
+{
+    if (!c || (count && (!d_in || !d_out))) return fail(LUTHE_E_PARAM, "bad argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(launch_ntt_inv(d_in, d_out, c->d_tw, count, (cudaStream_t)stream));
+    return LUTHE_OK;
+}
+extern "C" int luthe_ntt_mul(luthe_ctx *c, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, size_t count,
+                             void *stream)
+{
+    if (!c || (count && (!d_a || !d_b || !d_out))) return fail(LUTHE_E_PARAM, "bad argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(launch_ntt_mul(d_a, d_b, d_out, c->d_tw, count, (cudaStream_t)stream));
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_lwe_op(luthe_ctx *c, int op, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out,
+                            uint64_t imm, size_t count, void *stream)
+{
+    if (!c) return fail(LUTHE_E_PARAM, "null ctx");
+    if (op < LUTHE_OP_ADD || op > LUTHE_OP_MULS) return fail(LUTHE_E_PARAM, "unknown linear op %d", op);
+    const bool two = op == LUTHE_OP_ADD || op == LUTHE_OP_SUB || op == LUTHE_OP_MAC;
+    if (count && (!d_a || !d_out || (two && !d_b))) return fail(LUTHE_E_PARAM, "null buffer");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(launch_lwe_op(op, d_a, d_b, d_out, imm, count, (uint32_t)(c->p.glwe_dim * c->p.poly_size),
+                           (cudaStream_t)stream));
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_set_br_config(luthe_ctx *c, int g, int per_sm)
+{
+    if (!c) return fail(LUTHE_E_PARAM, "null ctx");
+    if (g < 1 || g > 2 || per_sm < 1) return fail(LUTHE_E_PARAM, "bad BR config %d/%d", g, per_sm);
+    BrConfig cfg{g, per_sm};
+    CUDA_TRY(cudaSetDevice(c->device));
+    size_t smem = br_smem_bytes(cfg, c->p.lwe_dim);
+    int max_smem = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device));
+    int blocks = (int)(max_smem / (smem + 1024));
+    if (blocks < per_sm) return fail(LUTHE_E_PARAM, "BR config %d/%d needs %zu B shared memory per CTA", g, per_sm,
+                                     smem);
+    drop_graphs(c);
+    c->br = cfg;
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_check_device_error(luthe_ctx *c)
+{
+    if (!c) return fail(LUTHE_E_PARAM, "null ctx");
+    uint32_t e = 0;
+    CUDA_TRY(cudaMemcpy(&e, c->d_err, 4, cudaMemcpyDeviceToHost));
+    if (e) {
+        cudaMemset(c->d_err, 0, 4);
+        return fail(LUTHE_E_TIMEOUT, "blind rotation: bounded wait for a BSK slab ran out");
+    }
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_autotune(luthe_ctx *c, size_t sample, char *json, size_t cap)
+{
+    int r = need_keys(c);
+    if (r) return r;
+    if (sample == 0) sample = (size_t)c->nsm * 4;
+    CUDA_TRY(cudaSetDevice(c->device));
+    const uint32_t n = c->p.lwe_dim;
+    uint32_t *d_l = nullptr, *d_ids = nullptr;
+    uint64_t *d_o = nullptr;
+    if ((r = dalloc(c, (void **)&d_l, sample * (n + 1) * 4))) return r;
+    if ((r = dalloc(c, (void **)&d_ids, sample * 4)) || (r = dalloc(c, (void **)&d_o, sample * (N + 1) * 8))) {
+        dfree(c, d_l, sample * (n + 1) * 4);
+        dfree(c, d_ids, sample * 4);
+        return r;
+    }
+    // deterministic pseudo-random mod-switched inputs
+    std::vector<uint32_t> hl(sample * (n + 1));
+    uint64_t st = 0x9E3779B97F4A7C15ull;
+    for (auto &v : hl) {
+        st ^= st << 13;
+        st ^= st >> 7;
+        st ^= st << 17;
+        v = (uint32_t)(st & (TWO_N - 1));
+    }
+    cudaMemcpy(d_l, hl.data(), hl.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemset(d_ids, 0, sample * 4);
+    const BrConfig cands[] = {{1, 1}, {2, 1}};
+    std::string rec = "{\"sample\":" + std::to_string(sample) + ",\"trials\":[";
+    float best = 1e30f;
+    BrConfig best_cfg = c->br;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    bool first = true;
+    for (const BrConfig &cfg : cands) {
+        size_t smem = br_smem_bytes(cfg, n);
+        int max_smem = 0;
+        cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
+        if ((size_t)max_smem < cfg.ctas_per_sm * (smem + 1024)) continue;
+        cudaError_t e = launch_blind_rotate(cfg, c->nsm, d_l, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_o,
+                                            sample, n, c->d_err, 0);
+        cudaEventRecord(e0, 0);
+        for (int rep = 0; rep < 2 && e == cudaSuccess; rep++)
+            e = launch_blind_rotate(cfg, c->nsm, d_l, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_o, sample, n,
+                                    c->d_err, 0);
+        cudaEventRecord(e1, 0);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            dfree(c, d_l, sample * (n + 1) * 4);
+            dfree(c, d_ids, sample * 4);
+            dfree(c, d_o, sample * (N + 1) * 8);
+            return fail(LUTHE_E_CUDA, "autotune: %s", cudaGetErrorString(e));
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= 2;
+        char buf[160];
+        snprintf(buf, sizeof buf, "%s{\"cts_per_cta\":%d,\"ctas_per_sm\":%d,\"ms\":%.4f,\"bootstraps_per_s\":%.1f}",
+                 first ? "" : ",", cfg.cts_per_cta, cfg.ctas_per_sm, ms, sample / (ms * 1e-3));
+        rec += buf;
+        first = false;
+        if (ms < best) {
+            best = ms;
+            best_cfg = cfg;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    dfree(c, d_l, sample * (n + 1) * 4);
+    dfree(c, d_ids, sample * 4);
+    dfree(c, d_o, sample * (N + 1) * 8);
+    drop_graphs(c);
+    c->br = best_cfg;
+    char tail[96];
+    snprintf(tail, sizeof tail, "],\"chosen\":{\"cts_per_cta\":%d,\"ctas_per_sm\":%d}}", best_cfg.cts_per_cta,
+             best_cfg.ctas_per_sm);
+    rec += tail;
+    if (json && cap) {
+        strncpy(json, rec.c_str(), cap - 1);
+        json[cap - 1] = 0;
+    }
+    return luthe_check_device_error(c);
+}

@@ -1,0 +1,133 @@
+// Goldilocks field arithmetic, p = 2^64 - 2^32 + 1, on the integer pipes.
+//
+// Values travel in "lazy" form: any u64 congruent to the residue (so in
+// [0, 2^64), possibly >= p).  add/sub/mul accept lazy inputs and return lazy
+// outputs; canon() brings a value to [0, p).  The reduction uses
+// 2^64 = 2^32 - 1 and 2^96 = -1 (mod p), the Solinas form that the reference
+// models in sw/solinas/solinas.py:218-319 and sw/ntt/ntt_gf64.sage:31-50.
+// Multiplication by 2^s is a shift plus that reduction: powers of two are the
+// 192-th roots of unity of this field (8 is a primitive 64-th root), which is
+// what makes the radix-32/radix-64 sub-transforms of the NTT multiply-free.
+#pragma once
+#include <stdint.h>
+
+typedef uint64_t u64;
+typedef uint32_t u32;
+
+namespace gl {
+
+constexpr u64 P = 0xFFFFFFFF00000001ull;
+constexpr u64 EPS = 0xFFFFFFFFull;  // 2^64 mod p
+
+__device__ __forceinline__ u64 add(u64 a, u64 b)
+{
+    u64 s = a + b;
+    u64 c = s < a ? EPS : 0ull;  // wrapped: +2^64 == +EPS
+    u64 t = s + c;
+    return t + (t < c ? EPS : 0ull);
+}
+
+__device__ __forceinline__ u64 sub(u64 a, u64 b)
+{
+    u64 d = a - b;
+    u64 c = a < b ? EPS : 0ull;  // borrowed: -2^64 == -EPS
+    u64 t = d - c;
+    return t - (d < c ? EPS : 0ull);
+}
+
+// lo + hi * 2^64  ->  lazy residue
+__device__ __forceinline__ u64 reduce128(u64 lo, u64 hi)
+{
+    u64 h1 = hi >> 32, h0 = hi & EPS;
+    u64 t = lo - h1;                    // h1 * 2^96 == -h1
+    t -= (lo < h1) ? EPS : 0ull;
+    u64 u = (h0 << 32) - h0;            // h0 * 2^64 == h0 * (2^32 - 1)
+    u64 r = t + u;
+    return r + (r < u ? EPS : 0ull);
+}
+
+__device__ __forceinline__ u64 mul(u64 a, u64 b) { return reduce128(a * b, __umul64hi(a, b)); }
+
+__device__ __forceinline__ u64 canon(u64 a) { return a >= P ? a - P : a; }
+
+__device__ __forceinline__ u64 neg(u64 a) { return sub(0ull, a); }
+
+__host__ __device__ constexpr int mod192(int s) { return ((s % 192) + 192) % 192; }
+
+// x * 2^S for a compile-time S (any sign; 2^192 == 1).
+template <int S>
+__device__ __forceinline__ u64 shl(u64 x)
+{
+    constexpr int s = mod192(S);
+    if constexpr (s == 0) {
+        return x;
+    } else if constexpr (s >= 96) {
+        return neg(shl<s - 96>(x));  // 2^96 == -1
+    } else if constexpr (s < 64) {
+        return reduce128(x << s, x >> (64 - s));
+    } else {
+        return shl<32>(shl<s - 32>(x));
+    }
+}
+
+// Cooley-Tukey butterfly: (u, v) <- (u + v 2^S, u - v 2^S)
+template <int S>
+__device__ __forceinline__ void ct_bf(u64 &u, u64 &v)
+{
+    constexpr int s = mod192(S);
+    if constexpr (s >= 96) {
+        u64 t = shl<s - 96>(v);
+        u64 a = sub(u, t);
+        v = add(u, t);
+        u = a;
+    } else {
+        u64 t = shl<s>(v);
+        u64 a = add(u, t);
+        v = sub(u, t);
+        u = a;
+    }
+}
+
+// Gentleman-Sande butterfly: (u, v) <- (u + v, (u - v) 2^S)
+template <int S>
+__device__ __forceinline__ void gs_bf(u64 &u, u64 &v)
+{
+    constexpr int s = mod192(S);
+    if constexpr (s >= 96) {
+        u64 a = add(u, v);
+        v = shl<s - 96>(sub(v, u));
+        u = a;
+    } else {
+        u64 a = add(u, v);
+        v = shl<s>(sub(u, v));
+        u = a;
+    }
+}
+
+// p -> 2^64 modulus switch of a canonical residue a:
+//   z = ((a * CST) >> 96) + bit95(a * CST),  CST = floor(2^160 / p) = 2^96 + 2^64 - 2
+// (hw/common_lib/.../mod_switch_to_2powerN.sv:62-64,132-134 with
+//  MOD_Q_W = 64, PRECISION_W = 96).
+__device__ __forceinline__ u64 modsw_p_to_q(u64 a)
+{
+    const u64 cst_lo = 0xFFFFFFFFFFFFFFFEull;  // CST mod 2^64; CST >> 64 = 2^32
+    u64 ph = __umul64hi(a, cst_lo);
+    u64 m = ph + (a << 32);
+    u64 top = (a >> 32) + (m < ph ? 1ull : 0ull);
+    return (top << 32) + (m >> 32) + ((m >> 31) & 1ull);
+}
+
+// Balanced decomposition, base 2^23, one level, of a 64-bit torus value,
+// embedded in Z_p (decomp_balseq_core.sv:135-150; the rounding and tie rule of
+// sw/decomposer/balanced_decomp_unfix_sign_round_bit.py:42-101 with bw=23, L=1).
+__device__ __forceinline__ u64 decomp23_to_p(u64 v)
+{
+    u64 rb = (v >> 40) & 1ull;
+    u64 c = (v >> 41) + rb;             // 0 .. 2^23
+    u64 t = c & 0x7FFFFFull;
+    bool negd = (t > 0x400000ull) || (t == 0x400000ull && rb);
+    // negative digit t - 2^23 embeds as p - (2^23 - t)
+    return negd ? (P - (0x800000ull - t)) : t;
+}
+
+}  // namespace gl

@@ -1,0 +1,582 @@
+// sm_100a kernels of the KS+PBS engine: BSK preparation, standalone NTTs,
+// the LWE key switch, the persistent blind rotation and the linear DOps.
+#include "kernels.cuh"
+#include "ntt.cuh"
+
+namespace luthe {
+
+using ntt::TPG;
+using ntt::POLY_WORDS;
+
+// ------------------------------------------------------------------ twiddles
+
+static uint64_t h_mulmod(uint64_t a, uint64_t b)
+{
+    unsigned __int128 x = (unsigned __int128)a * b;
+    return (uint64_t)(x % gl::P);
+}
+static uint64_t h_pow(uint64_t a, uint64_t e)
+{
+    uint64_t r = 1;
+    while (e) {
+        if (e & 1) r = h_mulmod(r, a);
+        a = h_mulmod(a, a);
+        e >>= 1;
+    }
+    return r;
+}
+// psi: primitive 4096-th root of unity with psi^64 = 8
+static const uint64_t PSI_4096 = 0x984ec5194d005735ull;
+
+void build_twiddles(uint64_t *tw)
+{
+    for (int s = 0; s < 8; s++)
+        for (int t = 0; t < TPG; t++) {
+            int k1 = ntt::a2_k1(t, s), j2 = t & 63;
+            uint64_t e = (uint64_t)(j2 * (2 * k1 + 1)) % TWO_N;
+            tw[s * TPG + t] = h_pow(PSI_4096, e);
+            tw[2048 + s * TPG + t] = h_pow(PSI_4096, (TWO_N - e) % TWO_N);
+        }
+}
+
+static const uint64_t N_INV = 0xffdfffff00200001ull;  // 2048^-1 mod p
+
+// ------------------------------------------------------------ BSK prepare
+//
+// One CTA per blind-rotation step i: the four standard-domain polynomials
+// BSK_i[row][col] (values < p) go through the forward NTT and are scaled by
+// N^-1 (the INTT's 1/N is folded here), then stored in the evaluation layout
+// of the BR kernel: slab[i][p][row][col][t], 64 KiB per step, so that a step's
+// slab is one contiguous bulk copy.
+__global__ void __launch_bounds__(256) bsk_prepare_kernel(const u64 *__restrict__ std_p, u64 *__restrict__ slab,
+                                                           const u64 *__restrict__ tw)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    u64 *buf = reinterpret_cast<u64 *>(smem_raw);
+    const int t = threadIdx.x;
+    const size_t i = blockIdx.x;
+    u64 x[4][8];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int e = 0; e < 8; e++) x[q][e] = std_p[(i * 4 + q) * N + ntt::coef_index(t, e)];
+    ntt::forward<4>(x, buf, tw, t, 1);
+#pragma unroll
+    for (int p = 0; p < 8; p++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) slab[((i * 8 + p) * 4 + q) * TPG + t] = gl::canon(gl::mul(x[q][p], N_INV));
+}
+
+cudaError_t launch_bsk_prepare(const uint64_t *d_std_p, uint64_t *d_slab, const uint64_t *d_tw, uint32_t n,
+                               cudaStream_t s)
+{
+    size_t smem = 4 * POLY_WORDS * 8;
+    cudaError_t e = cudaFuncSetAttribute(bsk_prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    bsk_prepare_kernel<<<n, TPG, smem, s>>>(d_std_p, d_slab, d_tw);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ standalone NTT
+//
+// G polynomials (or pairs) per CTA, 256 threads each; the twiddle tables are
+// staged once per CTA in shared memory.
+
+template <int G>
+__device__ __forceinline__ void load_tw(u64 *tws, const u64 *__restrict__ tw, int words)
+{
+    for (int i = threadIdx.x; i < words; i += G * TPG) tws[i] = tw[i];
+}
+
+// forward: coefficient order in, evaluation order k out (A_k = A(psi^{2k+1}))
+template <int G>
+__global__ void __launch_bounds__(G * 256) ntt_fwd_kernel(const u64 *__restrict__ in, u64 *__restrict__ out,
+                                                           const u64 *__restrict__ tw, size_t count)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    u64 *tws = reinterpret_cast<u64 *>(smem_raw);
+    u64 *buf = tws + 2048 + (threadIdx.x >> 8) * POLY_WORDS;
+    load_tw<G>(tws, tw, 2048);
+    __syncthreads();
+    const int t = threadIdx.x & 255, bar = 1 + (threadIdx.x >> 8);
+    for (size_t poly = (size_t)blockIdx.x * G + (threadIdx.x >> 8); poly < ((count + G - 1) / G) * G;
+         poly += (size_t)gridDim.x * G) {
+        const size_t src = poly < count ? poly : count - 1;
+        u64 x[1][8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) x[0][e] = in[src * N + ntt::coef_index(t, e)];
+        ntt::forward<1>(x, buf, tws, t, bar);
+        if (poly < count) {
+#pragma unroll
+            for (int p = 0; p < 8; p++) out[poly * N + ntt::eval_index(t, p)] = gl::canon(x[0][p]);
+        }
+        ntt::group_sync(bar);
+    }
+}
+
+// inverse: evaluation order in, coefficient order out, with the 1/N factor
+template <int G>
+__global__ void __launch_bounds__(G * 256) ntt_inv_kernel(const u64 *__restrict__ in, u64 *__restrict__ out,
+                                                           const u64 *__restrict__ tw, size_t count)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    u64 *tws = reinterpret_cast<u64 *>(smem_raw);
+    u64 *buf = tws + 2048 + (threadIdx.x >> 8) * POLY_WORDS;
+    load_tw<G>(tws, tw + 2048, 2048);
+    __syncthreads();
+    const int t = threadIdx.x & 255, bar = 1 + (threadIdx.x >> 8);
+    for (size_t poly = (size_t)blockIdx.x * G + (threadIdx.x >> 8); poly < ((count + G - 1) / G) * G;
+         poly += (size_t)gridDim.x * G) {
+        const size_t src = poly < count ? poly : count - 1;
+        u64 x[1][8];
+#pragma unroll
+        for (int p = 0; p < 8; p++) x[0][p] = gl::mul(in[src * N + ntt::eval_index(t, p)], N_INV);
+        ntt::inverse<1>(x, buf, tws, t, bar);
+        if (poly < count) {
+#pragma unroll
+            for (int e = 0; e < 8; e++) out[poly * N + ntt::coef_index(t, e)] = gl::canon(x[0][e]);
+        }
+        ntt::group_sync(bar);
+    }
+}
+
+// negacyclic product of pairs: INTT(NTT(a) * NTT(b))
+template <int G>
+__global__ void __launch_bounds__(G * 256) ntt_mul_kernel(const u64 *__restrict__ a, const u64 *__restrict__ b,
+                                                           u64 *__restrict__ out, const u64 *__restrict__ tw,
+                                                           size_t count)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    u64 *tws = reinterpret_cast<u64 *>(smem_raw);
+    u64 *buf = tws + 4096 + (threadIdx.x >> 8) * 2 * POLY_WORDS;
+    load_tw<G>(tws, tw, 4096);
+    __syncthreads();
+    const int t = threadIdx.x & 255, bar = 1 + (threadIdx.x >> 8);
+    for (size_t pr = (size_t)blockIdx.x * G + (threadIdx.x >> 8); pr < ((count + G - 1) / G) * G;
+         pr += (size_t)gridDim.x * G) {
+        const size_t src = pr < count ? pr : count - 1;
+        u64 x[2][8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            x[0][e] = a[src * N + ntt::coef_index(t, e)];
+            x[1][e] = b[src * N + ntt::coef_index(t, e)];
+        }
+        ntt::forward<2>(x, buf, tws, t, bar);
+        u64 r[1][8];
+#pragma unroll
+        for (int p = 0; p < 8; p++) r[0][p] = gl::mul(gl::mul(x[0][p], x[1][p]), N_INV);
+        ntt::group_sync(bar);
+        ntt::inverse<1>(r, buf, tws + 2048, t, bar);
+        if (pr < count) {
+#pragma unroll
+            for (int e = 0; e < 8; e++) out[pr * N + ntt::coef_index(t, e)] = gl::canon(r[0][e]);
+        }
+        ntt::group_sync(bar);
+    }
+}
+
+static int num_sms()
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+template <typename K>
+static cudaError_t launch_grid(K kernel, int G, size_t smem, size_t units, const void *const *args,
+                               cudaStream_t s)
+{
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, G * TPG, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    size_t want = (units + G - 1) / G;
+    size_t grid = (size_t)per_sm * num_sms();
+    if (grid > want) grid = want;
+    if (grid == 0) grid = 1;
+    return cudaLaunchKernel((const void *)kernel, dim3((unsigned)grid), dim3(G * TPG), (void **)args, smem, s);
+}
+
+cudaError_t launch_ntt_fwd(const uint64_t *d_in, uint64_t *d_out, const uint64_t *d_tw, size_t count,
+                           cudaStream_t s)
+{
+    if (count == 0) return cudaSuccess;
+    constexpr int G = 2;
+    const void *args[] = {&d_in, &d_out, &d_tw, &count};
+    return launch_grid(ntt_fwd_kernel<G>, G, (2048 + G * POLY_WORDS) * 8, count, args, s);
+}
+cudaError_t launch_ntt_inv(const uint64_t *d_in, uint64_t *d_out, const uint64_t *d_tw, size_t count,
+                           cudaStream_t s)
+{
+    if (count == 0) return cudaSuccess;
+    constexpr int G = 2;
+    const void *args[] = {&d_in, &d_out, &d_tw, &count};
+    return launch_grid(ntt_inv_kernel<G>, G, (2048 + G * POLY_WORDS) * 8, count, args, s);
+}
+cudaError_t launch_ntt_mul(const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, const uint64_t *d_tw,
+                           size_t count, cudaStream_t s)
+{
+    if (count == 0) return cudaSuccess;
+    constexpr int G = 2;
+    const void *args[] = {&d_a, &d_b, &d_out, &d_tw, &count};
+    return launch_grid(ntt_mul_kernel<G>, G, (4096 + G * 2 * POLY_WORDS) * 8, count, args, s);
+}
+
+// ---------------------------------------------------------------- key switch
+//
+// out21[c][x] = [x==n] b21 - sum_{y,z} d_{c,y,z} KSK[y][z][x]   (mod 2^21)
+// out2N[c][x] = round(out21 / 2^9) mod 2N
+// (pep_ks_blram_format.sv:158-172,240-243, pep_ks_mult_node.sv:95-104,
+//  pep_ks_out_process.sv:276-280,336-341).  A SIMT integer GEMM: M = ciphertexts,
+// N = output coefficients, K = (y, z) pairs.  The digits (in [-4, 4]) are made
+// on the fly from the 64-bit mask coefficients; 32-bit wrap-around keeps the
+// low 21 bits exact.  KSK is transposed to [y*L+z][x] on upload.
+__device__ __forceinline__ void ks_decomp(u64 v, int *d)
+{
+    // base 2^3, 6 levels: closest_rep = top 18 bits + round bit; tie rule of
+    // balanced_decomp_unfix_sign_round_bit.py:42-101 / decomp_parallel.sv:73-75,142-150
+    u32 rb = (u32)(v >> 45) & 1u;
+    u32 c = (u32)(v >> 46) + rb;  // 0 .. 2^18
+    u32 last_sign = ((c >> 17) & 1u) && ((c & 0x1FFFFu) || rb);
+    u32 carry = 0;
+#pragma unroll
+    for (int i = 0; i < KS_L; i++) {
+        u32 raw = (c >> (3 * i)) & 7u;
+        u32 nxt = (i + 1 < KS_L) ? ((c >> (3 * (i + 1))) & 7u) : (last_sign ? 7u : 0u);
+        u32 tv = raw + carry;
+        bool negd = (tv >> 3) || ((tv & 4u) && ((tv & 3u) || (nxt & 4u)));
+        d[i] = negd ? (int)tv - 8 : (int)tv;
+        carry = negd ? 1u : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, const u32 *__restrict__ ksk_t,
+                                                  u32 *__restrict__ out21, u32 *__restrict__ out2N, u32 B, u32 n,
+                                                  u32 xpad)
+{
+    __shared__ __align__(16) int dsm[KS_KC * KS_L][KS_BM];  // digits [k][ct]
+    __shared__ __align__(16) u32 ksm[KS_KC * KS_L][KS_BN];  // KSK tile [k][x]
+    const int tid = threadIdx.x;
+    const int ty = tid >> 5, tx = tid & 31;  // 8 x 4 cts, 32 x 4 outputs
+    const u32 c0 = blockIdx.y * KS_BM, x0 = blockIdx.x * KS_BN;
+    u32 acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = 0;
+
+    const int dct = tid >> 3, dy = tid & 7;  // decomposition role: 32 cts x 8 coefs
+    const u32 dct_g = min(c0 + dct, B - 1);
+    for (u32 y0 = 0; y0 < (u32)N; y0 += KS_KC) {
+        {
+            int d[KS_L];
+            ks_decomp(in[(size_t)dct_g * (N + 1) + y0 + dy], d);
+#pragma unroll
+            for (int z = 0; z < KS_L; z++) dsm[dy * KS_L + z][dct] = d[z];
+        }
+        const uint4 *src = reinterpret_cast<const uint4 *>(ksk_t + (size_t)y0 * KS_L * xpad + x0);
+#pragma unroll
+        for (int r = 0; r < (KS_KC * KS_L * KS_BN / 4) / 256; r++) {
+            int idx = tid + r * 256;
+            int k = idx / (KS_BN / 4), xv = idx % (KS_BN / 4);
+            reinterpret_cast<uint4 *>(&ksm[k][0])[xv] = src[(size_t)k * (xpad / 4) + xv];
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int k = 0; k < KS_KC * KS_L; k++) {
+            int4 dv = reinterpret_cast<const int4 *>(&dsm[k][0])[ty];
+            uint4 kv = reinterpret_cast<const uint4 *>(&ksm[k][0])[tx];
+            int dd[4] = {dv.x, dv.y, dv.z, dv.w};
+            u32 kk[4] = {kv.x, kv.y, kv.z, kv.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] += (u32)dd[i] * kk[j];
+        }
+        __syncthreads();
+    }
+    const u32 M = (1u << KS_W) - 1;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        u32 c = c0 + ty * 4 + i;
+        if (c >= B) continue;
+        u64 b = in[(size_t)c * (N + 1) + N];
+        u32 b21 = (u32)(((b >> (64 - KS_W)) + ((b >> (63 - KS_W)) & 1ull)) & M);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            u32 x = x0 + tx * 4 + j;
+            if (x > n) continue;
+            u32 v = (((x == n) ? b21 : 0u) - acc[i][j]) & M;
+            if (out21) out21[(size_t)c * (n + 1) + x] = v;
+            out2N[(size_t)c * (n + 1) + x] = ((v >> 9) + ((v >> 8) & 1u)) & (TWO_N - 1);
+        }
+    }
+}
+
+cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21, uint32_t *d_out2N,
+                             size_t B, uint32_t n, uint32_t xpad, cudaStream_t s)
+{
+    if (B == 0) return cudaSuccess;
+    dim3 grid(xpad / KS_BN, (unsigned)((B + KS_BM - 1) / KS_BM));
+    ks_kernel<<<grid, 256, 0, s>>>(d_in, d_ksk_t, d_out21, d_out2N, (u32)B, n, xpad);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------- blind rotation
+//
+// Persistent kernel: each CTA owns G ciphertexts at a time (256 threads each)
+// and runs all n steps for them; per step one 64 KiB BSK slab is fetched by a
+// bulk asynchronous copy into shared memory and read by every ciphertext of
+// the CTA.  The accumulator lives in registers (8 coefficients x 2 polys per
+// thread); shared memory carries the rotation gather and the NTT exchanges.
+// Step i (pe_pbs hot loop, feed_rot.sv:305-307, feed_final.sv:324,
+// decomp_balseq_core.sv:135-150, ntt_core_gf64, pp_core, mod_switch_to_2powerN,
+// acc_core.sv:8-12):
+//   diff_t = X^{a_i} ACC_t - ACC_t      (t = mask, body)
+//   d_t    = decomp_{2^23,1}(diff_t)    in Z_p
+//   R_col  = INTT( sum_row NTT(d_row) * BSK_i[row][col] )
+//   ACC_col += modsw_{p->2^64}(R_col)
+// then the sample extract of X^{-b} ACC (sxt_core.sv:8-14).
+
+constexpr unsigned long long MBAR_SPIN_LIMIT = 1ull << 26;
+
+__device__ __forceinline__ u32 smem_addr(const void *p) { return (u32)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(u64 *mbar, u32 count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mbar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(u64 *mbar, u32 bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, u32 bytes, u64 *mbar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+        : "memory");
+}
+// bounded wait on the given phase parity; returns false on timeout
+__device__ __forceinline__ bool mbar_wait(u64 *mbar, u32 parity)
+{
+    u32 a = smem_addr(mbar);
+    for (unsigned long long it = 0; it < MBAR_SPIN_LIMIT; it++) {
+        u32 done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void issue_slab(u64 *slab, const u64 *src, u64 *mbar)
+{
+    mbar_expect_tx(mbar, (u32)SLAB_BYTES);
+#pragma unroll
+    for (int c = 0; c < 4; c++) bulk_g2s(slab + c * (SLAB_WORDS / 4), src + c * (SLAB_WORDS / 4), SLAB_BYTES / 4, mbar);
+}
+
+template <int G>
+__global__ void __launch_bounds__(G * 256, 1)
+    br_kernel(const u32 *__restrict__ lwe2N, const u64 *__restrict__ luts, const u32 *__restrict__ lut_id, u32 nlut,
+              const u64 *__restrict__ bsk, const u64 *__restrict__ tw, u64 *__restrict__ out, u32 B, u32 n,
+              u32 *__restrict__ err)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    u64 *slab = reinterpret_cast<u64 *>(smem_raw);
+    u64 *tws = slab + SLAB_WORDS;
+    u64 *bufs = tws + 4096;
+    u64 *mbar = bufs + G * 2 * POLY_WORDS;
+    u32 *lwes = reinterpret_cast<u32 *>(mbar + 2);
+    const int g = threadIdx.x >> 8, t = threadIdx.x & 255, bar = 1 + g;
+    u64 *buf = bufs + g * 2 * POLY_WORDS;
+    u32 *my_lwe = lwes + g * (n + 1);
+
+    for (int i = threadIdx.x; i < 4096; i += G * TPG) tws[i] = tw[i];
+    if (threadIdx.x == 0) {
+        mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    u32 phase = 0;
+    const u32 ngroups = (B + G - 1) / G;
+    for (u32 grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+        const u32 cidx = grp * G + g;
+        const bool active = cidx < B;
+        const u32 ct = active ? cidx : B - 1;
+        for (u32 i = t; i <= n; i += TPG) my_lwe[i] = lwe2N[(size_t)ct * (n + 1) + i];
+        u32 lid = lut_id[ct];
+        if (lid >= nlut) lid = 0;  // host validates ids; keep the read in bounds regardless
+        const u64 *lut = luts + (size_t)lid * 2 * N;
+        u64 acc[2][8];
+#pragma unroll
+        for (int q = 0; q < 2; q++)
+#pragma unroll
+            for (int e = 0; e < 8; e++) acc[q][e] = lut[q * N + ntt::coef_index(t, e)];
+        if (threadIdx.x == 0) issue_slab(slab, bsk, mbar);
+        __syncthreads();
+
+        for (u32 i = 0; i < n; i++) {
+            const u32 a = my_lwe[i];
+            // feed: diff = X^a ACC - ACC, decomposed into Z_p
+#pragma unroll
+            for (int q = 0; q < 2; q++)
+#pragma unroll
+                for (int e = 0; e < 8; e++) buf[q * POLY_WORDS + ntt::coef_index(t, e)] = acc[q][e];
+            ntt::group_sync(bar);
+            u64 x[2][8];
+#pragma unroll
+            for (int q = 0; q < 2; q++)
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const u32 j = ntt::coef_index(t, e);
+                    const u32 src = (j + TWO_N - a) & (TWO_N - 1);
+                    u64 v = buf[q * POLY_WORDS + (src & (N - 1))];
+                    if (src >= (u32)N) v = 0ull - v;
+                    x[q][e] = gl::decomp23_to_p(v - acc[q][e]);
+                }
+            ntt::group_sync(bar);
+            ntt::forward<2>(x, buf, tws, t, bar);
+            // BSK multiply-accumulate in the evaluation domain
+            const bool ok = mbar_wait(mbar, phase);
+            phase ^= 1;
+            u64 r[2][8];
+#pragma unroll
+            for (int p = 0; p < 8; p++) {
+                const u64 *sb = slab + p * 4 * TPG + t;
+                const u64 b00 = sb[0], b01 = sb[TPG], b10 = sb[2 * TPG], b11 = sb[3 * TPG];
+                r[0][p] = gl::add(gl::mul(x[0][p], b00), gl::mul(x[1][p], b10));
+                r[1][p] = gl::add(gl::mul(x[0][p], b01), gl::mul(x[1][p], b11));
+            }
+            if (__syncthreads_or(!ok)) {
+                if (threadIdx.x == 0) atomicExch(err, 1u);
+                return;
+            }
+            if (threadIdx.x == 0 && i + 1 < n) issue_slab(slab, bsk + (size_t)(i + 1) * SLAB_WORDS, mbar);
+            ntt::inverse<2>(r, buf, tws + 2048, t, bar);
+#pragma unroll
+            for (int q = 0; q < 2; q++)
+#pragma unroll
+                for (int e = 0; e < 8; e++) acc[q][e] += gl::modsw_p_to_q(gl::canon(r[q][e]));
+            ntt::group_sync(bar);
+        }
+
+        // sample extract of coefficient 0 of X^{-b} ACC
+#pragma unroll
+        for (int q = 0; q < 2; q++)
+#pragma unroll
+            for (int e = 0; e < 8; e++) buf[q * POLY_WORDS + ntt::coef_index(t, e)] = acc[q][e];
+        ntt::group_sync(bar);
+        const u32 b = my_lwe[n];
+        if (active) {
+            u64 *o = out + (size_t)cidx * (N + 1);
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const u32 oi = t + 256 * m;
+                const u32 j = oi == 0 ? 0 : N - oi;
+                const u32 src = (j + b) & (TWO_N - 1);
+                u64 v = buf[src & (N - 1)];
+                if (src >= (u32)N) v = 0ull - v;
+                o[oi] = oi == 0 ? v : 0ull - v;
+            }
+            if (t == 0) {
+                const u32 src = b & (TWO_N - 1);
+                u64 v = buf[POLY_WORDS + (src & (N - 1))];
+                o[N] = src >= (u32)N ? 0ull - v : v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+size_t br_smem_bytes(const BrConfig &cfg, uint32_t n)
+{
+    const int G = cfg.cts_per_cta;
+    return (size_t)(SLAB_WORDS + 4096 + G * 2 * POLY_WORDS + 2) * 8 + (size_t)G * (n + 1) * 4;
+}
+
+template <int G>
+static cudaError_t br_attr(size_t smem)
+{
+    return cudaFuncSetAttribute(br_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n)
+{
+    size_t smem = br_smem_bytes(cfg, n);
+    switch (cfg.cts_per_cta) {
+    case 1: return br_attr<1>(smem);
+    case 2: return br_attr<2>(smem);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_lwe2N, const uint64_t *d_luts,
+                                const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
+                                uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s)
+{
+    if (B == 0) return cudaSuccess;
+    const int G = cfg.cts_per_cta;
+    size_t groups = (B + G - 1) / G;
+    size_t grid = (size_t)nsm * cfg.ctas_per_sm;
+    if (grid > groups) grid = groups;
+    size_t smem = br_smem_bytes(cfg, n);
+    u32 Bu = (u32)B;
+    void *args[] = {(void *)&d_lwe2N, (void *)&d_luts, (void *)&d_lut_id, (void *)&nlut, (void *)&d_bsk,
+                    (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err};
+    switch (G) {
+    case 1: return cudaLaunchKernel((const void *)br_kernel<1>, dim3((unsigned)grid), dim3(256), args, smem, s);
+    case 2: return cudaLaunchKernel((const void *)br_kernel<2>, dim3((unsigned)grid), dim3(512), args, smem, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---------------------------------------------------------- linear DOps
+//
+// pea_alu_core.sv:59-61,124-161: per coefficient, with the message constant
+// placed at the body only (imm << (64 - 5), 1 padding + 2 msg + 2 carry bits):
+//   ADD a+b, SUB a-b, MAC a*m+b, ADDS a+c, SUBS a-c, SSUB c-a, MULS a*m.
+__global__ void lwe_op_kernel(int op, const u64 *__restrict__ a, const u64 *__restrict__ b, u64 *__restrict__ o,
+                              u64 imm, size_t total, u32 dim)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const bool body = (i % (dim + 1)) == dim;
+        const u64 cst = body ? (imm << 59) : 0ull;
+        u64 v;
+        switch (op) {
+        case LWE_ADD: v = a[i] + b[i]; break;
+        case LWE_SUB: v = a[i] - b[i]; break;
+        case LWE_MAC: v = a[i] * imm + b[i]; break;
+        case LWE_ADDS: v = a[i] + cst; break;
+        case LWE_SUBS: v = a[i] - cst; break;
+        case LWE_SSUB: v = cst - a[i]; break;
+        default: v = a[i] * imm; break;
+        }
+        o[i] = v;
+    }
+}
+
+cudaError_t launch_lwe_op(int op, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, uint64_t imm,
+                          size_t count, uint32_t dim, cudaStream_t s)
+{
+    size_t total = count * (size_t)(dim + 1);
+    if (total == 0) return cudaSuccess;
+    size_t blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    lwe_op_kernel<<<(unsigned)blocks, 256, 0, s>>>(op, d_a, d_b, d_out, imm, total, dim);
+    return cudaGetLastError();
+}
+
+}  // namespace luthe

@@ -1,0 +1,48 @@
+// Launch wrappers for the sm_100a kernels of the KS+PBS engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+namespace luthe {
+
+constexpr int N = 2048;
+constexpr int TWO_N = 4096;
+constexpr int KS_L = 6;
+constexpr int KS_BL = 3;
+constexpr int KS_W = 21;
+constexpr int KS_BN = 128;                    // key-switch output tile
+constexpr int KS_BM = 32;                     // key-switch ciphertext tile
+constexpr int KS_KC = 8;                      // BLWE mask coefficients per K chunk
+constexpr int SLAB_WORDS = 8 * 4 * 256;       // one BR step of BSK: 2x2 polys of 2048
+constexpr size_t SLAB_BYTES = SLAB_WORDS * 8; // 64 KiB
+
+struct BrConfig {
+    int cts_per_cta;    // ciphertexts sharing one BSK slab per CTA (G)
+    int ctas_per_sm;    // resident CTAs per SM of the persistent grid
+};
+
+// device twiddle tables: [fwd 8x256][inv 8x256]
+void build_twiddles(uint64_t *host_tw /* 4096 words */);
+
+cudaError_t launch_bsk_prepare(const uint64_t *d_std_p, uint64_t *d_slab, const uint64_t *d_tw,
+                               uint32_t n, cudaStream_t s);
+cudaError_t launch_ntt_fwd(const uint64_t *d_in, uint64_t *d_out, const uint64_t *d_tw, size_t count,
+                           cudaStream_t s);
+cudaError_t launch_ntt_inv(const uint64_t *d_in, uint64_t *d_out, const uint64_t *d_tw, size_t count,
+                           cudaStream_t s);
+cudaError_t launch_ntt_mul(const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, const uint64_t *d_tw,
+                           size_t count, cudaStream_t s);
+cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21, uint32_t *d_out2N,
+                             size_t B, uint32_t n, uint32_t xpad, cudaStream_t s);
+cudaError_t launch_blind_rotate(const BrConfig &cfg, int num_sms, const uint32_t *d_lwe2N, const uint64_t *d_luts,
+                                const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
+                                uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s);
+size_t br_smem_bytes(const BrConfig &cfg, uint32_t n);
+cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n);
+
+enum LweOp : int { LWE_ADD = 0, LWE_SUB = 1, LWE_MAC = 2, LWE_ADDS = 3, LWE_SUBS = 4, LWE_SSUB = 5, LWE_MULS = 6 };
+cudaError_t launch_lwe_op(int op, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, uint64_t imm,
+                          size_t count, uint32_t dim, cudaStream_t s);
+
+}  // namespace luthe
