@@ -56,17 +56,20 @@ def bitrev(x, bits):
     return int(format(x, "0%db" % bits)[::-1], 2)
 
 
-def run_gtv(ref, name, n, N, per_batch, seed, noise):
+def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120):
     gtv = os.path.join(ref, "sw/bin/gtv/v1.4.1/gtv")
     out = tempfile.mkdtemp(prefix="gtv_")
     lwe_sd, glwe_sd = noise
-    cmd = [gtv, "--lwe-dim", str(n), "--glwe-dim", "1", "--poly-size", str(N), "--pbs-bl", "23", "--pbs-lc", "1",
+    # gtv searches for NTT roots unless given; pass the ones the reference's
+    # simulation flow uses (run.sh:429-458): phi = psi^(2048/N), omega = phi^2
+    phi = pow(0x984ec5194d005735, 2048 // N, P)
+    cmd = [gtv, "--omega-ru-n", str(phi * phi % P), "--phi-ru-2n", str(phi), "--lwe-dim", str(n), "--glwe-dim", "1", "--poly-size", str(N), "--pbs-bl", "23", "--pbs-lc", "1",
            "--ks-bl", "3", "--ks-lc", "6", "--ct-w", "64", "--ks-w", "21", "--msg-w", "2", "--carry-w", "2",
            "--pbs-batch", "1", "--pbs-per-batch", str(per_batch), "--seed", str(seed), "--ntt-radix", "2",
            "--psi", "4", "--ntt-delta", "3", "--lwe-std-dev", repr(lwe_sd), "--glwe-std-dev", repr(glwe_sd),
            "--ksk-pc", "1", "--bsk-pc", "1", "--ks-lbx", "1", "--ks-lby", "1", "--ks-lbz", "1",
            "--panic-on-failure", "--verbose", "-o", out]
-    log = subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=600).stdout
+    log = subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout).stdout
     d = os.path.realpath(os.path.join(out, "latest"))
     key = [int(x) for x in re.search(r"LweSecretKey \{ data: \[([^\]]*)\]", log).group(1).split(",")]
     msgs = [int(m) for m in re.findall(r"Generate Pbs_\d+ -> msg::(\d+)", log)]
@@ -112,8 +115,8 @@ def decomposer_vectors(ref):
         for i in range(L):
             base = (1 << (64 - tot)) * ((1 << (bw * i)) * (1 << (bw - 1)))
             vals += [base % 2**64, (base + (1 << (63 - tot))) % 2**64, (base - 1) % 2**64]
-        for top in range(1 << bw):
-            vals.append(((top << (64 - bw)) | (1 << (62 - tot))) % 2**64)
+        for top in range(min(1 << bw, 16)):
+            vals.append(((top << (64 - min(bw, 4))) | (1 << (62 - tot))) % 2**64)
         vals += [rng.getrandbits(64) for _ in range(4000)]
         digs = []
         for v in vals:
@@ -151,7 +154,8 @@ def solinas_vectors(ref):
     pos_max = 2 * 64 + 1
     exp_l = solinas.get_exponent(P)
     pos_d = solinas.get_position(exp_l, pos_max)
-    solinas.exp_l = exp_l  # compute_modulo reads this module global
+    solinas.exp_l = exp_l  # compute_modulo reads these module globals
+    solinas.MOD_W = 64
     rng = random.Random(13)
     vals = [0, 1, P - 1, P, P + 1, 2**64 - 1, 2**64, 2**96, 2**96 - 1, (P - 1) ** 2, 2**128 - 1]
     vals += [rng.getrandbits(64) * rng.getrandbits(64) for _ in range(3000)]
@@ -183,8 +187,10 @@ def modswitch_vectors():
 
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    run_gtv(ref, "n8_N64_noiseless", 8, 64, 4, 7, (0.0, 0.0))
-    run_gtv(ref, "n32_N256", 32, 256, 6, 11, (5.3943e-6, 4.4409e-16))
+    if "--models-only" not in sys.argv:
+        run_gtv(ref, "n8_N64_noiseless", 8, 64, 4, 7, (0.0, 0.0))
+        run_gtv(ref, "n32_N256", 32, 256, 6, 11, (5.3943e-6, 4.4409e-16))
+        run_gtv(ref, "n32_N2048", 32, 2048, 3, 13, (5.3943e-6, 4.4409e-16))
     decomposer_vectors(ref)
     monomial_vectors(ref)
     solinas_vectors(ref)
