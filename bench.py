@@ -1,0 +1,323 @@
+#!/usr/bin/env python3
+"""Benchmark of the batched KS+PBS hot path (TFHE n=804, k=1, N=2048, PBS 23x1,
+KS 3x6 mod 2^21, Goldilocks NTT) on B200.
+
+One step = one KS+PBS launch over the uneven batches 1+17+256+1000+4096
+(5370 BLWEs, each batch with its own random LUT), inputs resident in HBM.
+Prints one JSON line (rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's KS+PBS algorithm on the host cores: the
+reference's own CPU path is a prebuilt generator binary that is not shipped with
+this tree, so the CPU restatement of it (oracle/, same algorithm, all host
+threads) stands in, on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BATCHES = [1, 17, 256, 1000, 4096]
+METRIC = "KS+PBS bootstraps/s on 1 B200, batched vs plain, bit-exact; p50/p99 op latency"
+UNIT = "bootstraps/s"
+MODMUL_PER_BOOTSTRAP = 804 * 53248          # 4 NTT-class transforms + BSK MAC per BR step
+IMAD_PER_MODMUL = 4                         # 64x64->128 product as 4 32-bit IMAD
+KS_MAC_PER_BOOTSTRAP = 2048 * 6 * 805
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-sample", type=int, default=48, help="ciphertexts in the CPU-baseline sample")
+    ap.add_argument("--seed", type=int, default=20261203)
+    return ap.parse_args()
+
+
+def workload(L, params, keys, seed):
+    rng = np.random.default_rng(seed)
+    tables, msgs, ids = [], [], []
+    for b, size in enumerate(BATCHES):
+        tables.append(rng.integers(0, 16, 16).astype(np.uint32))
+        msgs.append(rng.integers(0, 16, size).astype(np.uint32))
+        ids.append(np.full(size, b, np.uint32))
+    msgs, ids = np.concatenate(msgs), np.concatenate(ids)
+    luts = np.stack([L.lut_build(params, t) for t in tables])
+    ct = L.encrypt(params, keys["glwe_key"], msgs, seed + 1)
+    expect = np.array([tables[i][m] for i, m in zip(ids, msgs)], np.uint32)
+    return ct, ids, luts, expect
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc, self.path = index, None, None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.path)
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        loaded = [s for s in sm if s > 0.5 * (max(sm) if sm else 0)]
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def read_traffic_per_bootstrap():
+    """DRAM bytes per bootstrap of the blind-rotation kernel from the committed
+    ncu summary (profiles/br_kernel_ncu.md, line 'dram_bytes_per_bootstrap: X')."""
+    path = os.path.join(ROOT, "profiles", "br_kernel_ncu.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("dram_bytes_per_bootstrap:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+def reference_arm(args):
+    import oracle
+    import luthe_b200 as L
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    params = L.default_params()
+    keys = L.keygen(params, args.seed)
+    ct, ids, luts, expect = workload(L, params, keys, args.seed)
+    ob = oracle.OracleBsk(keys["bsk"], params.lwe_dim, params.poly_size)
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    sample = max(1, min(args.cpu_sample, threads * 4))
+    times = []
+    for step in range(args.warmup + args.steps):
+        sl = slice((step * sample) % (len(ct) - sample), (step * sample) % (len(ct) - sample) + sample)
+        t0 = time.perf_counter()
+        out = ob.ks_pbs(keys["ksk"], ct[sl], luts, ids[sl])
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(dt)
+        assert np.array_equal(L.decrypt(params, keys["glwe_key"], out), expect[sl])
+    v = sample / statistics.mean(times)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": config_dict(),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{sample} BLWEs of the workload per step (KS+PBS), oracle/ CPU restatement"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def config_dict():
+    return {
+        "workload": "batched KS+PBS of uneven batches 1+17+256+1000+4096 = 5370 BLWEs in one launch, "
+                    "each batch its own random 4-bit LUT; TFHE n=804 k=1 N=2048 PBS 23x1 KS 3x6 mod 2^21, "
+                    "NTT mod 2^64-2^32+1",
+        "batches": BATCHES, "ciphertexts_per_step": sum(BATCHES),
+        "l2": "flushed between timed steps (256 MiB device write); BSK 52.7 MB and KSK 44 MB are L2-resident "
+              "by design inside a step",
+        "parallelism": "replicas (one independent engine per GPU, no collective on the data path)",
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    import luthe_b200 as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    params = L.default_params()
+    keys = L.keygen(params, args.seed)
+    ct, ids, luts, expect = workload(L, params, keys, args.seed)
+    B = len(ct)
+    eng = L.Engine(params, device=local)
+    eng.upload_keys(keys)
+    eng.upload_luts(luts)
+    tune = eng.autotune(592)
+    eng.reserve(B)
+
+    d_in = torch.from_numpy(ct.view(np.int64)).cuda()
+    d_ids = torch.from_numpy(ids.view(np.int32)).cuda()
+    d_out = torch.empty_like(d_in)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        eng.ks_pbs(d_in, d_ids, d_out, B, stream)
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        step()
+    torch.cuda.synchronize()
+    eng.check_device_error()
+    got = L.decrypt(params, keys["glwe_key"], d_out.cpu().numpy().view(np.uint64))
+    verified = bool(np.array_equal(got, expect))
+
+    # ---- timed region: K steps, L2 flushed between them (outside the events)
+    clocks = Clocks(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    evs = []
+    for k in range(args.steps):
+        flush.fill_(k)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = world * B * args.steps / (total_ms * 1e-3)
+
+    # ---- dominant kernel: the blind rotation alone, CUDA events on its stream
+    d_l2n = torch.empty((B, params.lwe_dim + 1), dtype=torch.int32, device="cuda")
+    eng.keyswitch(d_in, None, d_l2n, B, stream)
+    br_ms = []
+    for r in range(3):
+        flush.fill_(r)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.blind_rotate(d_l2n, d_ids, d_out, B, stream)
+        e1.record(stream)
+        e1.synchronize()
+        br_ms.append(e0.elapsed_time(e1))
+    br_s = statistics.median(br_ms) * 1e-3
+    imad_peak, glmul_peak = L.measure_int_peak(local)
+    achieved_imad = B * MODMUL_PER_BOOTSTRAP * IMAD_PER_MODMUL / br_s
+    traffic_pb = read_traffic_per_bootstrap()
+
+    # ---- plain path: one ciphertext per launch
+    plain_ms = []
+    one_in, one_id, one_out = d_in[:1], d_ids[:1], d_out[:1]
+    for r in range(8):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.ks_pbs(one_in, one_id, one_out, 1, stream)
+        e1.record(stream)
+        e1.synchronize()
+        if r >= 2:
+            plain_ms.append(e0.elapsed_time(e1))
+
+    # ---- end to end through the host-buffer API (pinned memory, copies timed)
+    h_in = torch.from_numpy(ct.view(np.int64)).pin_memory()
+    h_ids = torch.from_numpy(ids.view(np.int32)).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    hin, hid, hout = (h_in.numpy().view(np.uint64), h_ids.numpy().view(np.uint32), h_out.numpy().view(np.uint64))
+    eng.ks_pbs_host(hin, hid, hout)  # warm the staging buffers
+    e2e_ms = []
+    for r in range(max(2, min(args.steps, 3))):
+        flush.fill_(r)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        eng.ks_pbs_host(hin, hid, hout)
+        e1.record(torch.cuda.default_stream())
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_verified = bool(np.array_equal(L.decrypt(params, keys["glwe_key"], hout), expect))
+    e2e_val = world * B / (statistics.mean(e2e_ms) * 1e-3)
+
+    # ---- CPU baseline (rank 0, one GPU): the CPU restatement on all host cores
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_sample > 0:
+        import oracle
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        ob = oracle.OracleBsk(keys["bsk"], params.lwe_dim, params.poly_size)
+        s = min(args.cpu_sample, B)
+        t0 = time.perf_counter()
+        out = ob.ks_pbs(keys["ksk"], ct[:s], luts, ids[:s])
+        dt = time.perf_counter() - t0
+        gpu_first = d_out[:s].cpu().numpy().view(np.uint64)
+        cpu = {"value": s / dt, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"first {s} BLWEs of the workload, KS+PBS, {dt:.1f} s",
+               "bit_exact_vs_gpu": bool(np.array_equal(out, gpu_first))}
+
+    if rank == 0:
+        q = lambda xs, p: float(np.percentile(xs, p))
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": config_dict(),
+            "verified_decrypt": verified and e2e_verified,
+            "latency_ms": {"batch_step_p50": q(step_ms, 50), "batch_step_p99": q(step_ms, 99),
+                           "plain_p50": q(plain_ms, 50), "plain_p99": q(plain_ms, 99)},
+            "plain_bootstraps_per_s": 1e3 / statistics.mean(plain_ms),
+            "batched_over_plain": value / world / (1e3 / statistics.mean(plain_ms)),
+            "roofline": {"bound": "int", "kernel": "br_kernel", "achieved": achieved_imad / 1e12,
+                         "peak": imad_peak / 1e12, "unit": "TIMAD/s", "frac": achieved_imad / imad_peak,
+                         "peak_source": "measured live (luthe_measure_int_peak, 32-bit IMAD probe)",
+                         "work": f"{MODMUL_PER_BOOTSTRAP} modmul x {IMAD_PER_MODMUL} IMAD per bootstrap",
+                         "traffic": (traffic_pb * B if traffic_pb else None),
+                         "modmul_frac": B * MODMUL_PER_BOOTSTRAP / br_s / glmul_peak,
+                         "glmul_peak_per_s": glmul_peak, "br_ms": br_s * 1e3},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(ct.nbytes + ids.nbytes),
+                    "d2h_bytes_per_step": int(ct.nbytes), "ms_per_step": statistics.mean(e2e_ms)},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk,
+            "autotune": tune.get("chosen"),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -142,6 +142,11 @@ int luthe_autotune(luthe_ctx *ctx, size_t sample, char *json, size_t json_cap);
 /* Device-side error flag of the last blind rotation (bounded waits). */
 int luthe_check_device_error(luthe_ctx *ctx);
 
+/* Integer-pipe peaks of `device` measured by probe kernels: 32-bit IMAD per
+ * second and Goldilocks 64x64 multiply-reduce per second (the denominators of
+ * the integer roofline; no reference counterpart -- the HPU is an FPGA). */
+int luthe_measure_int_peak(int device, double *imad_per_s, double *glmul_per_s);
+
 /* ------------------------------------------------------------ host helpers */
 
 /* Seeded key generation (binary keys, Gaussian noise: LWE sigma 2^-17.5,

@@ -30,7 +30,7 @@ SYMBOLS = [
     "luthe_upload_bsk", "luthe_upload_ksk", "luthe_upload_luts", "luthe_reserve", "luthe_ks_pbs",
     "luthe_ks_pbs_host", "luthe_ks_pbs_graph", "luthe_keyswitch", "luthe_blind_rotate", "luthe_ntt_fwd",
     "luthe_ntt_inv", "luthe_ntt_mul", "luthe_lwe_op", "luthe_set_br_config", "luthe_autotune",
-    "luthe_check_device_error", "luthe_keygen", "luthe_encrypt", "luthe_decrypt", "luthe_lut_build",
+    "luthe_check_device_error", "luthe_measure_int_peak", "luthe_keygen", "luthe_encrypt", "luthe_decrypt", "luthe_lut_build",
 ]
 
 
@@ -86,6 +86,8 @@ def lib():
         L.luthe_set_br_config.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.luthe_autotune.argtypes = [vp, sz, ctypes.c_char_p, sz]
         L.luthe_check_device_error.argtypes = [vp]
+        L.luthe_measure_int_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_double)]
         L.luthe_keygen.argtypes = [P, u64, vp, vp, vp, vp]
         L.luthe_encrypt.argtypes = [P, vp, vp, sz, u64, vp]
         L.luthe_decrypt.argtypes = [P, vp, vp, sz, vp]
@@ -154,6 +156,13 @@ def lut_build(params, table):
     out = np.zeros(2 * params.poly_size, np.uint64)
     _check(lib().luthe_lut_build(ctypes.byref(params), _ptr(table), _ptr(out)))
     return out
+
+
+def measure_int_peak(device=0):
+    """(32-bit IMAD/s, Goldilocks mul/s) measured on `device` by probe kernels."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _check(lib().luthe_measure_int_peak(device, ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value
 
 
 # ------------------------------------------------------------------- engine
