@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-sample", type=int, default=48, help="ciphertexts in the CPU-baseline sample")
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="small profiling case: KS+PBS of 296 BLWEs (one persistent wave), twice, then exit")
     return ap.parse_args()
 
 
@@ -96,16 +98,22 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def read_traffic_per_bootstrap():
-    """DRAM bytes per bootstrap of the blind-rotation kernel from the committed
-    ncu summary (profiles/br_kernel_ncu.md, line 'dram_bytes_per_bootstrap: X')."""
+def read_traffic(B):
+    """DRAM bytes of one blind-rotation launch over B ciphertexts, from the
+    committed ncu summary (profiles/br_kernel_ncu.md): the BSK read once per
+    launch (fixed) plus the per-ciphertext input/output bytes, both measured on
+    the captured 296-ciphertext launch."""
     path = os.path.join(ROOT, "profiles", "br_kernel_ncu.md")
     if not os.path.exists(path):
         return None
+    vals = {}
     for line in open(path):
-        if line.strip().startswith("dram_bytes_per_bootstrap:"):
-            return float(line.split(":", 1)[1])
-    return None
+        k, _, v = line.partition(":")
+        if k.strip() in ("dram_bytes_fixed_per_launch", "dram_bytes_per_bootstrap"):
+            vals[k.strip()] = float(v)
+    if len(vals) < 2:
+        return None
+    return vals["dram_bytes_fixed_per_launch"] + vals["dram_bytes_per_bootstrap"] * B
 
 
 def reference_arm(args):
@@ -154,8 +162,34 @@ def config_dict():
     }
 
 
+def ncu_case():
+    """KS+PBS of 296 identity-LUT BLWEs twice (the case the ncu summaries under
+    profiles/ are captured on), checked by decryption."""
+    import torch
+    import luthe_b200 as L
+    p = L.default_params()
+    k = L.keygen(p, 3)
+    B = 296
+    with L.Engine(p) as e:
+        e.upload_keys(k)
+        e.upload_luts(L.lut_build(p, np.arange(16, dtype=np.uint32)))
+        ct = L.encrypt(p, k["glwe_key"], np.arange(B, dtype=np.uint32) % 16, 5)
+        d_in = torch.from_numpy(ct.view(np.int64)).cuda()
+        d_out = torch.empty_like(d_in)
+        ids = torch.zeros(B, dtype=torch.int32, device="cuda")
+        for _ in range(2):
+            e.ks_pbs(d_in, ids, d_out, B)
+        torch.cuda.synchronize()
+        e.check_device_error()
+        dec = L.decrypt(p, k["glwe_key"], d_out.cpu().numpy().view(np.uint64))
+    assert np.array_equal(dec, np.arange(B) % 16)
+    print("ncu case ok")
+
+
 def main():
     args = parse()
+    if args.ncu_case:
+        return ncu_case()
     if args.impl == "reference":
         return reference_arm(args)
     import torch
@@ -239,7 +273,7 @@ def main():
     br_s = statistics.median(br_ms) * 1e-3
     imad_peak, glmul_peak = L.measure_int_peak(local)
     achieved_imad = B * MODMUL_PER_BOOTSTRAP * IMAD_PER_MODMUL / br_s
-    traffic_pb = read_traffic_per_bootstrap()
+    traffic = read_traffic(B)
 
     # ---- plain path: one ciphertext per launch
     plain_ms = []
@@ -303,7 +337,7 @@ def main():
                          "peak": imad_peak / 1e12, "unit": "TIMAD/s", "frac": achieved_imad / imad_peak,
                          "peak_source": "measured live (luthe_measure_int_peak, 32-bit IMAD probe)",
                          "work": f"{MODMUL_PER_BOOTSTRAP} modmul x {IMAD_PER_MODMUL} IMAD per bootstrap",
-                         "traffic": (traffic_pb * B if traffic_pb else None),
+                         "traffic": traffic, "traffic_unit": "bytes per launch (ncu, scaled)",
                          "modmul_frac": B * MODMUL_PER_BOOTSTRAP / br_s / glmul_peak,
                          "glmul_peak_per_s": glmul_peak, "br_ms": br_s * 1e3},
             "cpu_baseline": cpu,

@@ -49,15 +49,19 @@ float time_probe(K kernel, T *buf, T seed, int blocks)
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     kernel<<<blocks, 256>>>(buf, seed);
-    cudaEventRecord(e0);
-    for (int r = 0; r < 5; r++) kernel<<<blocks, 256>>>(buf, seed + r);
-    cudaEventRecord(e1);
-    cudaEventSynchronize(e1);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
+    float best = 1e30f;
+    for (int round = 0; round < 3; round++) {  // best of three rounds of five launches
+        cudaEventRecord(e0);
+        for (int r = 0; r < 5; r++) kernel<<<blocks, 256>>>(buf, seed + r);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) best = ms;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    return ms / 5;
+    return best / 5;
 }
 
 }  // namespace
