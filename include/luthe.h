@@ -114,6 +114,18 @@ int luthe_ks_pbs_host(luthe_ctx *ctx, const uint64_t *h_in, const uint32_t *h_lu
 int luthe_ks_pbs_graph(luthe_ctx *ctx, const uint64_t *d_in, const uint32_t *d_lut_id, uint64_t *d_out,
                        size_t count, void *stream);
 
+/* luthe_ks_pbs for callers that must not allocate device memory while they run
+ * (allocator hooks and arenas, fixed-budget or framework-owned device memory).
+ * No counterpart in the reference.  It allocates nothing: the key-switched
+ * intermediate goes to a fixed 4 MiB array (2^20 u32) that every GPU loading
+ * this library holds until exit, so count * (n+1) must be <= 2^20 (1302
+ * ciphertexts at n = 804) or LUTHE_E_PARAM is returned.  The first call on a
+ * device looks up that array's device address; make that first call before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU
+ * race.  Keys and LUTs come from the context as for luthe_ks_pbs. */
+int luthe_ks_pbs_noalloc(luthe_ctx *ctx, const uint64_t *d_in, const uint32_t *d_lut_id, uint64_t *d_out,
+                         size_t count, void *stream);
+
 /* Stages on their own (pep_key_switch; pe_pbs BR + SXT). */
 int luthe_keyswitch(luthe_ctx *ctx, const uint64_t *d_in, uint32_t *d_out21, uint32_t *d_out2N, size_t count,
                     void *stream);

@@ -28,7 +28,7 @@ OP_ADD, OP_SUB, OP_MAC, OP_ADDS, OP_SUBS, OP_SSUB, OP_MULS = range(7)
 SYMBOLS = [
     "luthe_params_default", "luthe_last_error", "luthe_ctx_create", "luthe_ctx_destroy", "luthe_device_bytes",
     "luthe_upload_bsk", "luthe_upload_ksk", "luthe_upload_luts", "luthe_reserve", "luthe_ks_pbs",
-    "luthe_ks_pbs_host", "luthe_ks_pbs_graph", "luthe_keyswitch", "luthe_blind_rotate", "luthe_ntt_fwd",
+    "luthe_ks_pbs_host", "luthe_ks_pbs_graph", "luthe_ks_pbs_noalloc", "luthe_keyswitch", "luthe_blind_rotate", "luthe_ntt_fwd",
     "luthe_ntt_inv", "luthe_ntt_mul", "luthe_lwe_op", "luthe_set_br_config", "luthe_autotune",
     "luthe_check_device_error", "luthe_measure_int_peak", "luthe_keygen", "luthe_encrypt", "luthe_decrypt", "luthe_lut_build",
 ]
@@ -74,7 +74,7 @@ def lib():
         L.luthe_upload_ksk.argtypes = [vp, vp]
         L.luthe_upload_luts.argtypes = [vp, vp, u32]
         L.luthe_reserve.argtypes = [vp, sz]
-        for f in ("luthe_ks_pbs", "luthe_ks_pbs_graph"):
+        for f in ("luthe_ks_pbs", "luthe_ks_pbs_graph", "luthe_ks_pbs_noalloc"):
             getattr(L, f).argtypes = [vp, vp, vp, vp, sz, vp]
         L.luthe_ks_pbs_host.argtypes = [vp, vp, vp, vp, sz]
         L.luthe_keyswitch.argtypes = [vp, vp, vp, vp, sz, vp]
@@ -229,6 +229,11 @@ class Engine:
 
     def ks_pbs(self, d_in, d_ids, d_out, count, stream=None):
         _check(lib().luthe_ks_pbs(self._h, _ptr(d_in), _ptr(d_ids), _ptr(d_out), count, self._s(stream)))
+
+    def ks_pbs_noalloc(self, d_in, d_ids, d_out, count, stream=None):
+        """KS+PBS that allocates no device memory (fixed 4 MiB scratch; see
+        luthe_ks_pbs_noalloc in include/luthe.h for the limit and the sharing)."""
+        _check(lib().luthe_ks_pbs_noalloc(self._h, _ptr(d_in), _ptr(d_ids), _ptr(d_out), count, self._s(stream)))
 
     def ks_pbs_graph(self, d_in, d_ids, d_out, count, stream):
         _check(lib().luthe_ks_pbs_graph(self._h, _ptr(d_in), _ptr(d_ids), _ptr(d_out), count, self._s(stream)))

@@ -515,3 +515,55 @@ extern "C" int luthe_autotune(luthe_ctx *c, size_t sample, char *json, size_t ca
     }
     return luthe_check_device_error(c);
 }
+
+// ------------------------------------------------------------------------
+// KS+PBS without any device allocation.
+//
+// Some callers cannot call cudaMalloc while they run: code inside a memory
+// arena or allocator hook (a cudaMalloc there re-enters the allocator), code
+// running under a budget that forbids new device memory once it is set up, or
+// a host framework that owns all device memory and hands out only the buffers
+// it allocated.  For them, the key-switched intermediate (count x (n+1) u32)
+// lives in the fixed array below instead of the context's growable scratch.
+//
+// The array is 4 MiB and exists on every GPU that loads this library, for the
+// life of the process.  Every call shares it and it keeps the last call's
+// contents; the key switch overwrites every word the blind rotation then reads,
+// so nothing needs clearing between calls.  Calls that overlap on the GPU
+// (several streams, or several contexts on one device) race on it.
+static constexpr size_t NOALLOC_SCRATCH_WORDS = 1u << 20;
+static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_SCRATCH_WORDS];
+
+// In host code g_noalloc_scratch names a host-side stand-in, not device memory:
+// the kernels get the device address, looked up once per device with that
+// device current.
+static uint32_t *g_noalloc_addr[64];
+static bool g_noalloc_ready[64];
+
+extern "C" int luthe_ks_pbs_noalloc(luthe_ctx *c, const uint64_t *d_in, const uint32_t *d_ids, uint64_t *d_out,
+                                    size_t count, void *stream)
+{
+    int r = need_keys(c);
+    if (r) return r;
+    if (count == 0) return LUTHE_OK;
+    if (!d_in || !d_ids || !d_out) return fail(LUTHE_E_PARAM, "null buffer");
+    const size_t n1 = (size_t)c->p.lwe_dim + 1;
+    if (count > NOALLOC_SCRATCH_WORDS / n1)
+        return fail(LUTHE_E_PARAM, "luthe_ks_pbs_noalloc: %zu ciphertexts exceed the fixed scratch (at most %zu at n=%u)",
+                    count, NOALLOC_SCRATCH_WORDS / n1, c->p.lwe_dim);
+    if (c->device < 0 || c->device >= 64) return fail(LUTHE_E_PARAM, "device index %d out of range", c->device);
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (!g_noalloc_ready[c->device]) {
+        void *addr = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&addr, g_noalloc_scratch));
+        g_noalloc_addr[c->device] = (uint32_t *)addr;
+        g_noalloc_ready[c->device] = true;
+    }
+    uint32_t *scratch = g_noalloc_addr[c->device];
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t n = c->p.lwe_dim;
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, scratch, count, n, c->xpad, s));
+    CUDA_TRY(launch_blind_rotate(c->br, c->nsm, scratch, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out, count, n,
+                                 c->d_err, s));
+    return LUTHE_OK;
+}
