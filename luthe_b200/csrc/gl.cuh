@@ -19,31 +19,79 @@ namespace gl {
 constexpr u64 P = 0xFFFFFFFF00000001ull;
 constexpr u64 EPS = 0xFFFFFFFFull;  // 2^64 mod p
 
+// a + b: a 64-bit add whose carry (2^64 == EPS) is folded back at most twice;
+// written with explicit carry chains, which the compiler does not find from C.
 __device__ __forceinline__ u64 add(u64 a, u64 b)
 {
-    u64 s = a + b;
-    u64 c = s < a ? EPS : 0ull;  // wrapped: +2^64 == +EPS
-    u64 t = s + c;
-    return t + (t < c ? EPS : 0ull);
+    u64 r;
+    asm("{\n\t.reg .u32 c;\n\t.reg .u64 m;\n\t"
+        "add.cc.u64 %0, %1, %2;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "neg.s32 c, c;\n\t"
+        "cvt.u64.u32 m, c;\n\t"
+        "add.cc.u64 %0, %0, m;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "neg.s32 c, c;\n\t"
+        "cvt.u64.u32 m, c;\n\t"
+        "add.u64 %0, %0, m;\n\t}"
+        : "=l"(r)
+        : "l"(a), "l"(b));
+    return r;
 }
 
+// a - b: a borrow (-2^64 == -EPS) is folded back at most twice.
 __device__ __forceinline__ u64 sub(u64 a, u64 b)
 {
-    u64 d = a - b;
-    u64 c = a < b ? EPS : 0ull;  // borrowed: -2^64 == -EPS
-    u64 t = d - c;
-    return t - (d < c ? EPS : 0ull);
+    u64 r;
+    asm("{\n\t.reg .u32 c;\n\t.reg .u64 m;\n\t"
+        "sub.cc.u64 %0, %1, %2;\n\t"
+        "subc.u32 c, 0, 0;\n\t"
+        "cvt.u64.u32 m, c;\n\t"
+        "sub.cc.u64 %0, %0, m;\n\t"
+        "subc.u32 c, 0, 0;\n\t"
+        "cvt.u64.u32 m, c;\n\t"
+        "sub.u64 %0, %0, m;\n\t}"
+        : "=l"(r)
+        : "l"(a), "l"(b));
+    return r;
 }
 
-// lo + hi * 2^64  ->  lazy residue
+// lo + hi * 2^64  ->  lazy residue:  lo - h1 + h0 (2^32 - 1), hi = h1:h0
+// (h1 2^96 == -h1, h0 2^64 == h0 (2^32 - 1)); the h0 product goes to IMAD.
 __device__ __forceinline__ u64 reduce128(u64 lo, u64 hi)
 {
-    u64 h1 = hi >> 32, h0 = hi & EPS;
-    u64 t = lo - h1;                    // h1 * 2^96 == -h1
-    t -= (lo < h1) ? EPS : 0ull;
-    u64 u = (h0 << 32) - h0;            // h0 * 2^64 == h0 * (2^32 - 1)
-    u64 r = t + u;
-    return r + (r < u ? EPS : 0ull);
+    u64 r;
+    asm("{\n\t.reg .u32 c;\n\t.reg .u64 m, u, h;\n\t"
+        "cvt.u64.u32 h, %3;\n\t"
+        "sub.cc.u64 %0, %1, h;\n\t"
+        "subc.u32 c, 0, 0;\n\t"
+        "cvt.u64.u32 m, c;\n\t"
+        "sub.u64 %0, %0, m;\n\t"
+        "mul.wide.u32 u, %2, 0xFFFFFFFF;\n\t"
+        "add.cc.u64 %0, %0, u;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "neg.s32 c, c;\n\t"
+        "cvt.u64.u32 m, c;\n\t"
+        "add.u64 %0, %0, m;\n\t}"
+        : "=l"(r)
+        : "l"(lo), "r"((u32)hi), "r"((u32)(hi >> 32)));
+    return r;
+}
+
+// lo + h0 * 2^64 with h0 < 2^32: lo + h0 (2^32 - 1)
+__device__ __forceinline__ u64 reduce96(u64 lo, u32 h0)
+{
+    u64 r;
+    asm("{\n\t.reg .u32 c;\n\t.reg .u64 m, u;\n\t"
+        "mul.wide.u32 u, %2, 0xFFFFFFFF;\n\t"
+        "add.cc.u64 %0, %1, u;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "neg.s32 c, c;\n\t"
+        "cvt.u64.u32 m, c;\n\t"
+        "add.u64 %0, %0, m;\n\t}"
+        : "=l"(r)
+        : "l"(lo), "r"(h0));
+    return r;
 }
 
 __device__ __forceinline__ u64 mul(u64 a, u64 b) { return reduce128(a * b, __umul64hi(a, b)); }
@@ -63,6 +111,8 @@ __device__ __forceinline__ u64 shl(u64 x)
         return x;
     } else if constexpr (s >= 96) {
         return neg(shl<s - 96>(x));  // 2^96 == -1
+    } else if constexpr (s <= 32) {
+        return reduce96(x << s, (u32)(x >> (64 - s)));
     } else if constexpr (s < 64) {
         return reduce128(x << s, x >> (64 - s));
     } else {
