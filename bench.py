@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-sample", type=int, default=48, help="ciphertexts in the CPU-baseline sample")
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--ncu-case", action="store_true",
                     help="small profiling case: KS+PBS of 296 BLWEs (one persistent wave), twice, then exit")
     return ap.parse_args()
@@ -150,6 +151,85 @@ def reference_arm(args):
     }), flush=True)
 
 
+def rank_seed(seed, rank):
+    """Per-rank workload seed: replicas process independent ciphertexts."""
+    return seed + 1000003 * rank
+
+
+def max_over_ranks(x, dist, device):
+    """The slowest rank's value (timing is the max over ranks)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def serving(L, eng, params, keys, seed, n_req=400, rate=150.0):
+    """Serving loop under Poisson arrivals of 16-bit radix IOps (50 % ADD with
+    carry propagation, 30 % scalar compare, 20 % multiply); every result is
+    checked by decryption."""
+    from luthe_b200 import iops as I
+    eng.upload_luts(np.stack([L.lut_build(params, t) for t in I.lut_tables()]))
+    rng = np.random.default_rng(seed)
+    kinds = rng.choice(3, size=n_req, p=[0.5, 0.3, 0.2])
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    vals = rng.integers(0, 65536, (n_req, 2))
+    blocks, reqs, expect = [], [], []
+    for r in range(n_req):
+        a, b = int(vals[r, 0]), int(vals[r, 1])
+        if kinds[r] == 0:
+            reqs.append([I.prog_add(), 16, 8])
+            expect.append((a + b) % 65536)
+            blocks += I.to_blocks(a) + I.to_blocks(b)
+        elif kinds[r] == 1:
+            reqs.append([I.prog_cmp_gt(b), 8, 1])
+            expect.append(int(a > b))
+            blocks += I.to_blocks(a)
+        else:
+            reqs.append([I.prog_mul(), 16, 8])
+            expect.append((a * b) % 65536)
+            blocks += I.to_blocks(a) + I.to_blocks(b)
+    ct = L.encrypt(params, keys["glwe_key"], np.array(blocks, np.uint32), seed + 7)
+    off = 0
+    for r in reqs:
+        r[1], off = ct[off:off + r[1]], off + r[1]
+    srv = L.Server(eng, pool_bytes=4 << 30, max_pbs=4096)
+    srv.run([tuple(reqs[0]), tuple(reqs[1])])          # warm-up
+    base = srv.counters()
+    ids, outs, lat = [None] * n_req, {}, {}
+    t0 = time.perf_counter()
+    sub = 0
+    while len(outs) < n_req:
+        now = time.perf_counter() - t0
+        while sub < n_req and arrivals[sub] <= now:
+            ids[sub] = srv.submit(*reqs[sub])
+            sub += 1
+        if sub == len(outs):
+            time.sleep(max(0.0, min(0.002, arrivals[sub] - now)))
+            continue
+        srv.step()
+        for r in range(sub):
+            if r not in outs:
+                got = srv.fetch(ids[r], reqs[r][2])
+                if got is not None:
+                    outs[r], lat[r] = got[0], got[1]
+    wall = time.perf_counter() - t0
+    cnt = {k: v - base[k] for k, v in srv.counters().items()}
+    srv.close()
+    ok = 0
+    for r in range(n_req):
+        dec = [int(x) for x in L.decrypt(params, keys["glwe_key"], outs[r])]
+        ok += (I.from_blocks(dec) if reqs[r][2] == 8 else dec[0]) == expect[r]
+    ls = np.array([lat[r] for r in range(n_req)]) * 1e3
+    return {"requests": n_req, "arrival_rate_per_s": rate, "mix": "50% add, 30% scalar cmp, 20% mul (16-bit radix)",
+            "throughput_requests_per_s": n_req / wall, "pbs_per_s": cnt["pbs"] / wall,
+            "latency_ms_p50": float(np.percentile(ls, 50)), "latency_ms_p99": float(np.percentile(ls, 99)),
+            "rounds": cnt["rounds"], "pbs": cnt["pbs"], "alu_dops": cnt["alu"], "launches": cnt["launches"],
+            "results_decrypt_correct": f"{ok}/{n_req}"}
+
+
 def config_dict():
     return {
         "workload": "batched KS+PBS of uneven batches 1+17+256+1000+4096 = 5370 BLWEs in one launch, "
@@ -207,7 +287,7 @@ def main():
 
     params = L.default_params()
     keys = L.keygen(params, args.seed)
-    ct, ids, luts, expect = workload(L, params, keys, args.seed)
+    ct, ids, luts, expect = workload(L, params, keys, rank_seed(args.seed, rank))
     B = len(ct)
     eng = L.Engine(params, device=local)
     eng.upload_keys(keys)
@@ -249,11 +329,8 @@ def main():
     torch.cuda.synchronize()
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(step_ms)
+    total_ms = max_over_ranks(sum(step_ms), dist, "cuda")
     if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
     ms_per_step = total_ms / args.steps
     value = world * B * args.steps / (total_ms * 1e-3)
@@ -304,7 +381,10 @@ def main():
         e1.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
     e2e_verified = bool(np.array_equal(L.decrypt(params, keys["glwe_key"], hout), expect))
-    e2e_val = world * B / (statistics.mean(e2e_ms) * 1e-3)
+    e2e_val = world * B / (max_over_ranks(statistics.mean(e2e_ms), dist, "cuda") * 1e-3)
+
+    # ---- serving loop (one GPU): Poisson arrivals of radix IOps
+    serve = serving(L, eng, params, keys, args.seed + 99) if world == 1 and not args.no_serving else None
 
     # ---- CPU baseline (rank 0, one GPU): the CPU restatement on all host cores
     cpu = None
@@ -346,6 +426,7 @@ def main():
             "gpu_launches": 2 * args.steps,
             "clocks": clk,
             "autotune": tune.get("chosen"),
+            "serving": serve,
         }
         print(json.dumps(line), flush=True)
     eng.close()

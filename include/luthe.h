@@ -109,6 +109,13 @@ int luthe_ks_pbs(luthe_ctx *ctx, const uint64_t *d_in, const uint32_t *d_lut_id,
  * Pinned host memory gives the full PCIe/C2C bandwidth. */
 int luthe_ks_pbs_host(luthe_ctx *ctx, const uint64_t *h_in, const uint32_t *h_lut_id, uint64_t *h_out,
                       size_t count);
+/* Many-LUT PBS (PBS_ML2/ML4/ML8, docs/dop.md:101-121): one blind rotation per
+ * ciphertext, `mlk` outputs per ciphertext written to rows count_index*mlk+m.
+ * The LUT packs the mlk functions in consecutive blocks of 2^(msg+carry)/mlk
+ * boxes (luthe_lut_build of the concatenated tables); inputs must stay below
+ * 2^(msg+carry)/mlk. */
+int luthe_ks_pbs_ml(luthe_ctx *ctx, const uint64_t *d_in, const uint32_t *d_lut_id, uint64_t *d_out, size_t count,
+                    uint32_t mlk, void *stream);
 /* CUDA-graph form of luthe_ks_pbs: the first call for a given (pointers,
  * count, stream) captures the launches, later calls replay the graph. */
 int luthe_ks_pbs_graph(luthe_ctx *ctx, const uint64_t *d_in, const uint32_t *d_lut_id, uint64_t *d_out,
@@ -143,6 +150,31 @@ int luthe_ntt_mul(luthe_ctx *ctx, const uint64_t *d_a, const uint64_t *d_b, uint
 /* Linear DOps on `count` BLWEs (pe_alu). */
 int luthe_lwe_op(luthe_ctx *ctx, int op, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, uint64_t imm,
                  size_t count, void *stream);
+
+/* ---------------------------------------------------------- serving loop
+ *
+ * Continuous batching of DOp programs (the firmware's IOp -> DOp expansion,
+ * fw/ublaze/src/ucore_fw.c:54-130, and the instruction scheduler,
+ * hw/module/instruction_scheduler): a request is a DOp program (32-bit words
+ * in the field layouts of fw/ublaze/src/hpu_dop_fmt.h:49-117) over its own
+ * 128-register file, with n_src input blocks (LD Rx TS.slot) and n_dst output
+ * blocks (ST TD.slot Rx).  Opcodes: ADD 0x01 SUB 0x02 MAC 0x05 ADDS 0x09
+ * SUBS 0x0A SSUB 0x0B MULS 0x0C SYNC 0x10 LD 0x20 ST 0x21 PBS 0x30
+ * PBS_ML2/4/8 0x31-0x33 (| 0x08: flush variant).  Each luthe_server_step
+ * admits pending requests while the slot pool (carved from the context's HBM
+ * budget) has room, issues every ready linear DOp of every request in one
+ * launch and every ready PBS of every request in one KS+PBS launch, and
+ * retires finished requests.  Latency is measured from submit to retire. */
+typedef struct luthe_server luthe_server;
+int luthe_server_create(luthe_ctx *ctx, uint64_t pool_bytes, uint32_t max_pbs, luthe_server **out);
+void luthe_server_destroy(luthe_server *srv);
+int luthe_server_submit(luthe_server *srv, const uint32_t *dops, uint32_t n_dops, const uint64_t *h_src,
+                        uint32_t n_src, uint32_t n_dst, uint64_t *id);
+int luthe_server_step(luthe_server *srv, uint32_t *n_completed, uint32_t *n_active, uint32_t *n_pending);
+/* Copy a finished request's output blocks out and release it; LUTHE_E_STATE
+ * while it is not finished. */
+int luthe_server_fetch(luthe_server *srv, uint64_t id, uint64_t *h_dst, double *latency_s, double *queue_s);
+int luthe_server_counters(luthe_server *srv, uint64_t *rounds, uint64_t *pbs, uint64_t *alu, uint64_t *launches);
 
 /* Blind-rotation launch shape: ciphertexts per CTA sharing one BSK slab (1 or
  * 2) and CTAs per SM of the persistent grid.  luthe_autotune times the

@@ -28,7 +28,9 @@ OP_ADD, OP_SUB, OP_MAC, OP_ADDS, OP_SUBS, OP_SSUB, OP_MULS = range(7)
 SYMBOLS = [
     "luthe_params_default", "luthe_last_error", "luthe_ctx_create", "luthe_ctx_destroy", "luthe_device_bytes",
     "luthe_upload_bsk", "luthe_upload_ksk", "luthe_upload_luts", "luthe_reserve", "luthe_ks_pbs",
-    "luthe_ks_pbs_host", "luthe_ks_pbs_graph", "luthe_ks_pbs_noalloc", "luthe_keyswitch", "luthe_blind_rotate", "luthe_ntt_fwd",
+    "luthe_ks_pbs_host", "luthe_ks_pbs_graph", "luthe_ks_pbs_noalloc", "luthe_ks_pbs_ml", "luthe_keyswitch",
+    "luthe_server_create", "luthe_server_destroy", "luthe_server_submit", "luthe_server_step",
+    "luthe_server_fetch", "luthe_server_counters", "luthe_blind_rotate", "luthe_ntt_fwd",
     "luthe_ntt_inv", "luthe_ntt_mul", "luthe_lwe_op", "luthe_set_br_config", "luthe_autotune",
     "luthe_check_device_error", "luthe_measure_int_peak", "luthe_keygen", "luthe_encrypt", "luthe_decrypt", "luthe_lut_build",
 ]
@@ -77,6 +79,14 @@ def lib():
         for f in ("luthe_ks_pbs", "luthe_ks_pbs_graph", "luthe_ks_pbs_noalloc"):
             getattr(L, f).argtypes = [vp, vp, vp, vp, sz, vp]
         L.luthe_ks_pbs_host.argtypes = [vp, vp, vp, vp, sz]
+        L.luthe_ks_pbs_ml.argtypes = [vp, vp, vp, vp, sz, u32, vp]
+        pu32, pu64, pd = ctypes.POINTER(u32), ctypes.POINTER(u64), ctypes.POINTER(ctypes.c_double)
+        L.luthe_server_create.argtypes = [vp, u64, u32, ctypes.POINTER(vp)]
+        L.luthe_server_destroy.argtypes = [vp]
+        L.luthe_server_submit.argtypes = [vp, vp, u32, vp, u32, u32, pu64]
+        L.luthe_server_step.argtypes = [vp, pu32, pu32, pu32]
+        L.luthe_server_fetch.argtypes = [vp, u64, vp, pd, pd]
+        L.luthe_server_counters.argtypes = [vp, pu64, pu64, pu64, pu64]
         L.luthe_keyswitch.argtypes = [vp, vp, vp, vp, sz, vp]
         L.luthe_blind_rotate.argtypes = [vp, vp, vp, vp, sz, vp]
         L.luthe_ntt_fwd.argtypes = [vp, vp, vp, sz, vp]
@@ -230,6 +240,10 @@ class Engine:
     def ks_pbs(self, d_in, d_ids, d_out, count, stream=None):
         _check(lib().luthe_ks_pbs(self._h, _ptr(d_in), _ptr(d_ids), _ptr(d_out), count, self._s(stream)))
 
+    def ks_pbs_ml(self, d_in, d_ids, d_out, count, mlk, stream=None):
+        """Many-LUT PBS: row c*mlk+m of d_out is function m of input c."""
+        _check(lib().luthe_ks_pbs_ml(self._h, _ptr(d_in), _ptr(d_ids), _ptr(d_out), count, mlk, self._s(stream)))
+
     def ks_pbs_noalloc(self, d_in, d_ids, d_out, count, stream=None):
         """KS+PBS that allocates no device memory (fixed 4 MiB scratch; see
         luthe_ks_pbs_noalloc in include/luthe.h for the limit and the sharing)."""
@@ -274,3 +288,71 @@ class Engine:
 
     def check_device_error(self):
         _check(lib().luthe_check_device_error(self._h))
+
+
+class Server:
+    """Serving loop over an :class:`Engine`: DOp programs (see :mod:`luthe_b200.iops`)
+    are submitted as requests and executed with continuous batching; ready PBS
+    DOps of all in-flight requests share one KS+PBS launch per round."""
+
+    def __init__(self, engine, pool_bytes=1 << 30, max_pbs=4096):
+        self.engine = engine
+        self.N = engine.params.poly_size
+        h = ctypes.c_void_p()
+        _check(lib().luthe_server_create(engine._h, pool_bytes, max_pbs, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().luthe_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, dops, src_blocks, n_dst):
+        """Queue a request; returns its id.  src_blocks: [n_src][N+1] u64 BLWEs."""
+        dops = np.ascontiguousarray(dops, np.uint32)
+        src = np.ascontiguousarray(src_blocks, np.uint64).reshape(-1, self.N + 1)
+        rid = ctypes.c_uint64()
+        _check(lib().luthe_server_submit(self._h, _ptr(dops), dops.size, _ptr(src) if src.size else None,
+                                         src.shape[0], n_dst, ctypes.byref(rid)))
+        return rid.value
+
+    def step(self):
+        """One scheduling round; returns (completed, active, pending)."""
+        c, a, p = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib().luthe_server_step(self._h, ctypes.byref(c), ctypes.byref(a), ctypes.byref(p)))
+        return c.value, a.value, p.value
+
+    def fetch(self, rid, n_dst):
+        """(output blocks, latency s, queueing s) of a finished request, or None."""
+        out = np.zeros((n_dst, self.N + 1), np.uint64)
+        lat, q = ctypes.c_double(), ctypes.c_double()
+        code = lib().luthe_server_fetch(self._h, rid, _ptr(out), ctypes.byref(lat), ctypes.byref(q))
+        if code == E_STATE:
+            return None
+        _check(code)
+        return out, lat.value, q.value
+
+    def counters(self):
+        v = [ctypes.c_uint64() for _ in range(4)]
+        _check(lib().luthe_server_counters(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(zip(("rounds", "pbs", "alu", "launches"), (x.value for x in v)))
+
+    def run(self, requests):
+        """Submit all requests [(dops, src, n_dst)] now and step until done;
+        returns the output blocks in submission order."""
+        ids = [self.submit(*r) for r in requests]
+        outs = {}
+        while len(outs) < len(ids):
+            self.step()
+            for rid, r in zip(ids, requests):
+                if rid not in outs:
+                    got = self.fetch(rid, r[2])
+                    if got is not None:
+                        outs[rid] = got[0]
+        return [outs[i] for i in ids]

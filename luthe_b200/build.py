@@ -16,7 +16,7 @@ ORACLE_LIB = os.path.join(ROOT, "oracle", "liboracle.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["kernels.cu", "api.cu", "probe.cu", "keygen.cpp"]
+SOURCES = ["kernels.cu", "api.cu", "serve.cu", "probe.cu", "keygen.cpp"]
 
 
 def _newer(target, deps):

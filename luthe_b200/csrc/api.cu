@@ -9,12 +9,13 @@
 #include <vector>
 #include "../../include/luthe.h"
 #include "kernels.cuh"
+#include "ctx.h"
 
 using namespace luthe;
 
-static thread_local char g_err[512] = "";
+thread_local char g_err[512] = "";
 
-static int fail(int code, const char *fmt, ...)
+int fail(int code, const char *fmt, ...)
 {
     va_list ap;
     va_start(ap, fmt);
@@ -22,44 +23,6 @@ static int fail(int code, const char *fmt, ...)
     va_end(ap);
     return code;
 }
-#define CUDA_TRY(expr)                                                                    \
-    do {                                                                                  \
-        cudaError_t e_ = (expr);                                                          \
-        if (e_ != cudaSuccess)                                                            \
-            return fail(LUTHE_E_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_),    \
-                        __FILE__, __LINE__);                                              \
-    } while (0)
-
-struct GraphEntry {
-    const void *in, *ids;
-    void *out;
-    size_t count;
-    cudaStream_t stream;
-    cudaGraphExec_t exec;
-};
-
-struct luthe_ctx {
-    luthe_params p;
-    int device = 0;
-    int nsm = 148;
-    uint64_t budget = 0, used = 0;
-    uint64_t *d_tw = nullptr;     // [2][8][256]
-    uint64_t *d_bsk = nullptr;    // [n][8][2][2][256]
-    uint32_t *d_ksk = nullptr;    // [kN*L][xpad]
-    uint32_t xpad = 0;
-    uint64_t *d_luts = nullptr;   // [nlut][2][N]
-    uint32_t nlut = 0;
-    uint32_t *d_err = nullptr;
-    // scratch
-    uint32_t *d_lwe2N = nullptr;  // [cap][n+1]
-    size_t cap = 0;
-    // host-path staging
-    uint64_t *d_hin = nullptr, *d_hout = nullptr;
-    uint32_t *d_hids = nullptr;
-    size_t hcap = 0;
-    BrConfig br{2, 1};
-    std::vector<GraphEntry> graphs;
-};
 
 extern "C" const char *luthe_last_error(void) { return g_err; }
 
@@ -89,7 +52,7 @@ static int check_params(const luthe_params *p)
     return LUTHE_OK;
 }
 
-static int dalloc(luthe_ctx *c, void **ptr, size_t bytes)
+int dalloc(luthe_ctx *c, void **ptr, size_t bytes)
 {
     if (c->used + bytes > c->budget)
         return fail(LUTHE_E_BUDGET, "HBM budget exceeded: %llu + %zu > %llu bytes", (unsigned long long)c->used,
@@ -98,7 +61,7 @@ static int dalloc(luthe_ctx *c, void **ptr, size_t bytes)
     c->used += bytes;
     return LUTHE_OK;
 }
-static void dfree(luthe_ctx *c, void *ptr, size_t bytes)
+void dfree(luthe_ctx *c, void *ptr, size_t bytes)
 {
     if (ptr) {
         cudaFree(ptr);
@@ -106,7 +69,7 @@ static void dfree(luthe_ctx *c, void *ptr, size_t bytes)
     }
 }
 
-static void drop_graphs(luthe_ctx *c)
+void drop_graphs(luthe_ctx *c)
 {
     for (auto &g : c->graphs) cudaGraphExecDestroy(g.exec);
     c->graphs.clear();
@@ -219,7 +182,7 @@ extern "C" int luthe_upload_luts(luthe_ctx *c, const uint64_t *h, uint32_t count
     return LUTHE_OK;
 }
 
-static int ensure_scratch(luthe_ctx *c, size_t count)
+int ensure_scratch(luthe_ctx *c, size_t count)
 {
     if (count <= c->cap) return LUTHE_OK;
     drop_graphs(c);
@@ -240,7 +203,7 @@ extern "C" int luthe_reserve(luthe_ctx *c, size_t max_count)
     return ensure_scratch(c, max_count);
 }
 
-static int need_keys(luthe_ctx *c)
+int need_keys(luthe_ctx *c)
 {
     if (!c) return fail(LUTHE_E_PARAM, "null ctx");
     if (!c->d_bsk || !c->d_ksk) return fail(LUTHE_E_STATE, "keys not uploaded");
@@ -268,6 +231,24 @@ extern "C" int luthe_ks_pbs(luthe_ctx *c, const uint64_t *d_in, const uint32_t *
     CUDA_TRY(cudaSetDevice(c->device));
     if ((r = ensure_scratch(c, count))) return r;
     return enqueue_ks_pbs(c, d_in, d_ids, d_out, count, (cudaStream_t)stream);
+}
+
+extern "C" int luthe_ks_pbs_ml(luthe_ctx *c, const uint64_t *d_in, const uint32_t *d_ids, uint64_t *d_out,
+                               size_t count, uint32_t mlk, void *stream)
+{
+    int r = need_keys(c);
+    if (r) return r;
+    if (mlk != 1 && mlk != 2 && mlk != 4 && mlk != 8) return fail(LUTHE_E_PARAM, "many-LUT factor %u not in {1,2,4,8}", mlk);
+    if (count == 0) return LUTHE_OK;
+    if (!d_in || !d_ids || !d_out) return fail(LUTHE_E_PARAM, "null buffer");
+    CUDA_TRY(cudaSetDevice(c->device));
+    if ((r = ensure_scratch(c, count))) return r;
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t n = c->p.lwe_dim;
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s));
+    CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out, count,
+                                 n, c->d_err, s, nullptr, mlk));
+    return LUTHE_OK;
 }
 
 extern "C" int luthe_ks_pbs_graph(luthe_ctx *c, const uint64_t *d_in, const uint32_t *d_ids, uint64_t *d_out,

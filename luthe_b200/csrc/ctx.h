@@ -1,0 +1,54 @@
+// Internal: the context shared by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <vector>
+#include "../../include/luthe.h"
+#include "kernels.cuh"
+
+struct GraphEntry {
+    const void *in, *ids;
+    void *out;
+    size_t count;
+    cudaStream_t stream;
+    cudaGraphExec_t exec;
+};
+
+struct luthe_ctx {
+    luthe_params p;
+    int device = 0;
+    int nsm = 148;
+    uint64_t budget = 0, used = 0;
+    uint64_t *d_tw = nullptr;     // [2][8][256]
+    uint64_t *d_bsk = nullptr;    // [n][8][2][2][256]
+    uint32_t *d_ksk = nullptr;    // [kN*L][xpad]
+    uint32_t xpad = 0;
+    uint64_t *d_luts = nullptr;   // [nlut][2][N]
+    uint32_t nlut = 0;
+    uint32_t *d_err = nullptr;
+    // scratch
+    uint32_t *d_lwe2N = nullptr;  // [cap][n+1]
+    size_t cap = 0;
+    // host-path staging
+    uint64_t *d_hin = nullptr, *d_hout = nullptr;
+    uint32_t *d_hids = nullptr;
+    size_t hcap = 0;
+    luthe::BrConfig br{2, 1};
+    std::vector<GraphEntry> graphs;
+};
+
+extern thread_local char g_err[512];
+int fail(int code, const char *fmt, ...);
+int dalloc(luthe_ctx *c, void **ptr, size_t bytes);
+void dfree(luthe_ctx *c, void *ptr, size_t bytes);
+void drop_graphs(luthe_ctx *c);
+int ensure_scratch(luthe_ctx *c, size_t count);
+int need_keys(luthe_ctx *c);
+
+#define CUDA_TRY(expr)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (expr);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(LUTHE_E_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_),    \
+                        __FILE__, __LINE__);                                              \
+    } while (0)

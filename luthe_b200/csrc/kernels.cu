@@ -253,9 +253,9 @@ __device__ __forceinline__ void ks_decomp(u64 v, int *d)
     }
 }
 
-__global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, const u32 *__restrict__ ksk_t,
-                                                  u32 *__restrict__ out21, u32 *__restrict__ out2N, u32 B, u32 n,
-                                                  u32 xpad)
+__global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, const u32 *__restrict__ src_idx,
+                                                  const u32 *__restrict__ ksk_t, u32 *__restrict__ out21,
+                                                  u32 *__restrict__ out2N, u32 B, u32 n, u32 xpad)
 {
     __shared__ __align__(16) int dsm[KS_KC * KS_L][KS_BM];  // digits [k][ct]
     __shared__ __align__(16) u32 ksm[KS_KC * KS_L][KS_BN];  // KSK tile [k][x]
@@ -269,7 +269,8 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
         for (int j = 0; j < 4; j++) acc[i][j] = 0;
 
     const int dct = tid >> 3, dy = tid & 7;  // decomposition role: 32 cts x 8 coefs
-    const u32 dct_g = min(c0 + dct, B - 1);
+    const u32 dct_c = min(c0 + dct, B - 1);
+    const size_t dct_g = src_idx ? src_idx[dct_c] : dct_c;  // row of the input array
     for (u32 y0 = 0; y0 < (u32)N; y0 += KS_KC) {
         {
             int d[KS_L];
@@ -303,7 +304,7 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
     for (int i = 0; i < 4; i++) {
         u32 c = c0 + ty * 4 + i;
         if (c >= B) continue;
-        u64 b = in[(size_t)c * (N + 1) + N];
+        u64 b = in[(size_t)(src_idx ? src_idx[c] : c) * (N + 1) + N];
         u32 b21 = (u32)(((b >> (64 - KS_W)) + ((b >> (63 - KS_W)) & 1ull)) & M);
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -317,11 +318,11 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
 }
 
 cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21, uint32_t *d_out2N,
-                             size_t B, uint32_t n, uint32_t xpad, cudaStream_t s)
+                             size_t B, uint32_t n, uint32_t xpad, cudaStream_t s, const uint32_t *d_src_idx)
 {
     if (B == 0) return cudaSuccess;
     dim3 grid(xpad / KS_BN, (unsigned)((B + KS_BM - 1) / KS_BM));
-    ks_kernel<<<grid, 256, 0, s>>>(d_in, d_ksk_t, d_out21, d_out2N, (u32)B, n, xpad);
+    ks_kernel<<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, (u32)B, n, xpad);
     return cudaGetLastError();
 }
 
@@ -391,7 +392,7 @@ template <int G>
 __global__ void __launch_bounds__(G * 256, 1)
     br_kernel(const u32 *__restrict__ lwe2N, const u64 *__restrict__ luts, const u32 *__restrict__ lut_id, u32 nlut,
               const u64 *__restrict__ bsk, const u64 *__restrict__ tw, u64 *__restrict__ out, u32 B, u32 n,
-              u32 *__restrict__ err)
+              u32 *__restrict__ err, const u32 *__restrict__ dst_idx, u32 mlk)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     u64 *slab = reinterpret_cast<u64 *>(smem_raw);
@@ -473,28 +474,33 @@ __global__ void __launch_bounds__(G * 256, 1)
             ntt::group_sync(bar);
         }
 
-        // sample extract of coefficient 0 of X^{-b} ACC
+        // sample extract of coefficient 0 of X^{-b} ACC.  Many-LUT (mlk = 2, 4, 8
+        // functions packed in one LUT, docs/dop.md:113-121): output m extracts
+        // coefficient m*N/mlk, i.e. coefficient 0 of X^{-(b + m N/mlk)} ACC,
+        // into consecutive output rows.
 #pragma unroll
         for (int q = 0; q < 2; q++)
 #pragma unroll
             for (int e = 0; e < 8; e++) buf[q * POLY_WORDS + ntt::coef_index(t, e)] = acc[q][e];
         ntt::group_sync(bar);
-        const u32 b = my_lwe[n];
         if (active) {
-            u64 *o = out + (size_t)cidx * (N + 1);
+            const size_t row0 = dst_idx ? dst_idx[cidx] : (size_t)cidx * mlk;
+            for (u32 m = 0; m < mlk; m++) {
+                const u32 b = (my_lwe[n] + m * (N / mlk)) & (TWO_N - 1);
+                u64 *o = out + (row0 + m) * (N + 1);
 #pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const u32 oi = t + 256 * m;
-                const u32 j = oi == 0 ? 0 : N - oi;
-                const u32 src = (j + b) & (TWO_N - 1);
-                u64 v = buf[src & (N - 1)];
-                if (src >= (u32)N) v = 0ull - v;
-                o[oi] = oi == 0 ? v : 0ull - v;
-            }
-            if (t == 0) {
-                const u32 src = b & (TWO_N - 1);
-                u64 v = buf[POLY_WORDS + (src & (N - 1))];
-                o[N] = src >= (u32)N ? 0ull - v : v;
+                for (int r = 0; r < 8; r++) {
+                    const u32 oi = t + 256 * r;
+                    const u32 j = oi == 0 ? 0 : N - oi;
+                    const u32 src = (j + b) & (TWO_N - 1);
+                    u64 v = buf[src & (N - 1)];
+                    if (src >= (u32)N) v = 0ull - v;
+                    o[oi] = oi == 0 ? v : 0ull - v;
+                }
+                if (t == 0) {
+                    u64 v = buf[POLY_WORDS + (b & (N - 1))];
+                    o[N] = b >= (u32)N ? 0ull - v : v;
+                }
             }
         }
         __syncthreads();
@@ -525,9 +531,11 @@ cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n)
 
 cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_lwe2N, const uint64_t *d_luts,
                                 const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
-                                uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s)
+                                uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s,
+                                const uint32_t *d_dst_idx, uint32_t mlk)
 {
     if (B == 0) return cudaSuccess;
+    if (mlk != 1 && mlk != 2 && mlk != 4 && mlk != 8) return cudaErrorInvalidValue;
     const int G = cfg.cts_per_cta;
     size_t groups = (B + G - 1) / G;
     size_t grid = (size_t)nsm * cfg.ctas_per_sm;
@@ -535,7 +543,8 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
     size_t smem = br_smem_bytes(cfg, n);
     u32 Bu = (u32)B;
     void *args[] = {(void *)&d_lwe2N, (void *)&d_luts, (void *)&d_lut_id, (void *)&nlut, (void *)&d_bsk,
-                    (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err};
+                    (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err,
+                    (void *)&d_dst_idx, (void *)&mlk};
     switch (G) {
     case 1: return cudaLaunchKernel((const void *)br_kernel<1>, dim3((unsigned)grid), dim3(256), args, smem, s);
     case 2: return cudaLaunchKernel((const void *)br_kernel<2>, dim3((unsigned)grid), dim3(512), args, smem, s);
@@ -566,6 +575,44 @@ __global__ void lwe_op_kernel(int op, const u64 *__restrict__ a, const u64 *__re
         }
         o[i] = v;
     }
+}
+
+// A batch of linear DOps (and register copies) over a pool of BLWE slots:
+// op i writes slot dst[i] from slots a[i], b[i] and the immediate imm[i]
+// (the serving loop issues every ready ALU DOp of every request in one launch).
+__global__ void alu_batch_kernel(const AluOp *__restrict__ ops, u64 *__restrict__ pool, u32 nops, u32 dim)
+{
+    const size_t w = dim + 1, total = (size_t)nops * w;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const AluOp o = ops[i / w];
+        const size_t c = i % w;
+        const bool body = c == dim;
+        const u64 cst = body ? (o.imm << 59) : 0ull;
+        const u64 a = pool[(size_t)o.a * w + c];
+        const u64 b = (o.op == LWE_ADD || o.op == LWE_SUB || o.op == LWE_MAC) ? pool[(size_t)o.b * w + c] : 0ull;
+        u64 v;
+        switch (o.op) {
+        case LWE_ADD: v = a + b; break;
+        case LWE_SUB: v = a - b; break;
+        case LWE_MAC: v = a * o.imm + b; break;
+        case LWE_ADDS: v = a + cst; break;
+        case LWE_SUBS: v = a - cst; break;
+        case LWE_SSUB: v = cst - a; break;
+        case LWE_MULS: v = a * o.imm; break;
+        default: v = a; break;  // copy
+        }
+        pool[(size_t)o.dst * w + c] = v;
+    }
+}
+
+cudaError_t launch_alu_batch(const AluOp *d_ops, uint64_t *d_pool, uint32_t nops, uint32_t dim, cudaStream_t s)
+{
+    if (nops == 0) return cudaSuccess;
+    size_t total = (size_t)nops * (dim + 1);
+    size_t blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    alu_batch_kernel<<<(unsigned)blocks, 256, 0, s>>>(d_ops, d_pool, nops, dim);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_lwe_op(int op, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, uint64_t imm,

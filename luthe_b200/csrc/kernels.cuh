@@ -34,14 +34,24 @@ cudaError_t launch_ntt_inv(const uint64_t *d_in, uint64_t *d_out, const uint64_t
 cudaError_t launch_ntt_mul(const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, const uint64_t *d_tw,
                            size_t count, cudaStream_t s);
 cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21, uint32_t *d_out2N,
-                             size_t B, uint32_t n, uint32_t xpad, cudaStream_t s);
+                             size_t B, uint32_t n, uint32_t xpad, cudaStream_t s,
+                             const uint32_t *d_src_idx = nullptr);
 cudaError_t launch_blind_rotate(const BrConfig &cfg, int num_sms, const uint32_t *d_lwe2N, const uint64_t *d_luts,
                                 const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
-                                uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s);
+                                uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s,
+                                const uint32_t *d_dst_idx = nullptr, uint32_t mlk = 1);
 size_t br_smem_bytes(const BrConfig &cfg, uint32_t n);
 cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n);
 
 enum LweOp : int { LWE_ADD = 0, LWE_SUB = 1, LWE_MAC = 2, LWE_ADDS = 3, LWE_SUBS = 4, LWE_SSUB = 5, LWE_MULS = 6 };
+// one linear DOp or register copy (op = LWE_COPY) on slots of a BLWE pool
+constexpr int LWE_COPY = 7;
+struct AluOp {
+    uint32_t op, dst, a, b;
+    uint64_t imm;
+};
+cudaError_t launch_alu_batch(const AluOp *d_ops, uint64_t *d_pool, uint32_t nops, uint32_t dim, cudaStream_t s);
+
 cudaError_t launch_lwe_op(int op, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, uint64_t imm,
                           size_t count, uint32_t dim, cudaStream_t s);
 

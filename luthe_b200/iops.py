@@ -1,0 +1,263 @@
+"""Radix-integer IOps as DOp programs for the serving loop.
+
+The reference expands integer operations (IOps, docs/iop.md) into digit
+operations (DOps, docs/dop.md) in its firmware and TFHE-rs backend (the DOp
+programs themselves are not in the reference).  Here the expansion is written
+from the documented semantics: a 16-bit integer is 8 blocks (digits) of a
+2-bit message with 2 carry bits of headroom and a padding bit; ALU DOps are
+exact on the payload while it stays below 16; a PBS applies a 16-entry LUT and
+cleans the noise.  Programs are 32-bit DOp words in the field layouts of
+fw/ublaze/src/hpu_dop_fmt.h:49-117 (opcodes: include/luthe.h).
+
+    ADD      a + b mod 2^16: blockwise ADD, then a carry chain of PBS_ML2
+             (message and carry of a block from one blind rotation)
+    CMP_GT   a > k for a clear 16-bit k: per-block sign PBS, a 3-level tree of
+             bivariate combine PBS (MSB block decides), a final PBS to {0, 1}
+    MUL      a * b mod 2^16: schoolbook digit products (bivariate PBS on
+             MAC-packed a_i * 4 + b_j, low and high halves), then per-column
+             carry-save reduction in groups of up to 5 terms
+"""
+import numpy as np
+
+BLOCKS = 8
+MSG_BITS = 2
+OPC = dict(ADD=0x01, SUB=0x02, MAC=0x05, ADDS=0x09, SUBS=0x0A, SSUB=0x0B, MULS=0x0C, SYNC=0x10, LD=0x20, ST=0x21,
+           PBS=0x30, PBS_ML2=0x31, PBS_ML4=0x32, PBS_ML8=0x33)
+MEM_HEAP, MEM_SRC, MEM_DST = 1, 2, 3
+
+# ------------------------------------------------------------------ LUTs
+# 16-entry tables on the 4-bit payload x = carry*4 + msg (docs/dop.md:136-159 aliases)
+
+
+def _many(*fs):
+    """Many-LUT table: k functions of an input < 16/k, packed in consecutive blocks."""
+    k = len(fs)
+    span = 16 // k
+    return [fs[b // span](b % span) for b in range(16)]
+
+
+LUTS = {
+    "None": [x for x in range(16)],
+    "MsgOnly": [x & 3 for x in range(16)],
+    "CarryInMsg": [x >> 2 for x in range(16)],
+    "MultCarryMsgLsb": [((x >> 2) * (x & 3)) & 3 for x in range(16)],
+    "MultCarryMsgMsb": [((x >> 2) * (x & 3)) >> 2 for x in range(16)],
+    "ManyCarryMsg": _many(lambda x: x & 3, lambda x: x >> 2),
+    "CmpCombine": [(x >> 2) if (x >> 2) != 1 else (x & 3) for x in range(16)],
+    "IsTwo": [1 if x == 2 else 0 for x in range(16)],
+}
+for _k in range(4):
+    LUTS[f"Cmp{_k}"] = [0 if (x & 3) < _k else 1 if (x & 3) == _k else 2 for x in range(16)]
+LUT_NAMES = list(LUTS)
+LUT_ID = {name: i for i, name in enumerate(LUT_NAMES)}
+
+
+def lut_tables():
+    """[nlut][16] tables in LUT-id order (upload with luthe_lut_build per table)."""
+    return [LUTS[name] for name in LUT_NAMES]
+
+
+# ------------------------------------------------------------- assembler
+
+def enc_arith(op, dst, s0, s1=0, mul=0):
+    return (OPC[op] << 26) | ((mul & 0x1F) << 21) | ((s1 & 0x7F) << 14) | ((s0 & 0x7F) << 7) | (dst & 0x7F)
+
+
+def enc_arith_msg(op, dst, s0, cst):
+    return (OPC[op] << 26) | ((cst & 0x7FF) << 15) | ((s0 & 0x7F) << 7) | (dst & 0x7F)
+
+
+def enc_mem(op, rid, mode, slot):
+    return (OPC[op] << 26) | ((slot & 0xFFFF) << 10) | ((mode & 3) << 8) | (rid & 0x7F)
+
+
+def enc_pbs(op, dst, src, gid):
+    return (OPC[op] << 26) | ((gid & 0xFFF) << 14) | ((src & 0x7F) << 7) | (dst & 0x7F)
+
+
+class Program:
+    """DOp program builder with a register allocator over the 128-entry file."""
+
+    def __init__(self, n_src, n_dst):
+        self.words = []
+        self.n_src, self.n_dst = n_src, n_dst
+        self.free = list(range(127, -1, -1))
+
+    def reg(self):
+        return self.free.pop()
+
+    def pair(self, k=2):
+        """k consecutive registers starting at a multiple of k (many-LUT destination)."""
+        for base in range(0, 128, k):
+            if all(r in self.free for r in range(base, base + k)):
+                for r in range(base, base + k):
+                    self.free.remove(r)
+                return base
+        raise RuntimeError("register file exhausted")
+
+    def release(self, *rs):
+        for r in rs:
+            if r not in self.free:
+                self.free.append(r)
+
+    def ld(self, r, src_block):
+        self.words.append(enc_mem("LD", r, MEM_SRC, src_block))
+
+    def st(self, dst_block, r):
+        self.words.append(enc_mem("ST", r, MEM_DST, dst_block))
+
+    def add(self, d, a, b):
+        self.words.append(enc_arith("ADD", d, a, b))
+
+    def mac(self, d, a, b, f):
+        self.words.append(enc_arith("MAC", d, a, b, f))
+
+    def pbs(self, d, s, lut):
+        self.words.append(enc_pbs("PBS", d, s, LUT_ID[lut]))
+
+    def pbs_ml2(self, d, s, lut):
+        self.words.append(enc_pbs("PBS_ML2", d, s, LUT_ID[lut]))
+
+    def array(self):
+        return np.array(self.words, np.uint32)
+
+
+def prog_add():
+    """a (src blocks 0..7) + b (src 8..15) -> dst blocks 0..7, mod 2^16."""
+    p = Program(2 * BLOCKS, BLOCKS)
+    a = [p.reg() for _ in range(BLOCKS)]
+    b = [p.reg() for _ in range(BLOCKS)]
+    for i in range(BLOCKS):
+        p.ld(a[i], i)
+        p.ld(b[i], BLOCKS + i)
+    carry = None
+    for i in range(BLOCKS):
+        p.add(a[i], a[i], b[i])                   # <= 6
+        p.release(b[i])
+        if carry is not None:
+            p.add(a[i], a[i], carry)              # <= 7
+            p.release(carry)
+        if i < BLOCKS - 1:
+            d = p.pair(2)
+            p.pbs_ml2(d, a[i], "ManyCarryMsg")    # d: msg, d+1: carry
+            p.st(i, d)
+            p.release(d, a[i])
+            carry = d + 1
+        else:
+            d = p.reg()
+            p.pbs(d, a[i], "MsgOnly")
+            p.st(i, d)
+    return p.array()
+
+
+def prog_cmp_gt(k):
+    """a (src blocks 0..7) > k (clear 16-bit) -> dst block 0 in {0, 1}."""
+    p = Program(BLOCKS, 1)
+    a = [p.reg() for _ in range(BLOCKS)]
+    for i in range(BLOCKS):
+        p.ld(a[i], i)
+    cmp = []
+    for i in range(BLOCKS):
+        d = p.reg()
+        p.pbs(d, a[i], f"Cmp{(k >> (2 * i)) & 3}")
+        cmp.append(d)
+        p.release(a[i])
+    while len(cmp) > 1:                           # cmp[i]: block i, higher index = more significant
+        nxt = []
+        for lo, hi in zip(cmp[0::2], cmp[1::2]):
+            x = p.reg()
+            p.mac(x, hi, lo, 4)                   # hi * 4 + lo <= 10
+            d = p.reg()
+            p.pbs(d, x, "CmpCombine")
+            p.release(x, hi, lo)
+            nxt.append(d)
+        cmp = nxt
+    d = p.reg()
+    p.pbs(d, cmp[0], "IsTwo")
+    p.st(0, d)
+    return p.array()
+
+
+def prog_mul():
+    """a (src 0..7) * b (src 8..15) -> dst blocks 0..7, mod 2^16."""
+    p = Program(2 * BLOCKS, BLOCKS)
+    a = [p.reg() for _ in range(BLOCKS)]
+    b = [p.reg() for _ in range(BLOCKS)]
+    for i in range(BLOCKS):
+        p.ld(a[i], i)
+        p.ld(b[i], BLOCKS + i)
+    cols = [[] for _ in range(BLOCKS)]
+    for k in range(BLOCKS):
+        for i in range(k + 1):                    # digit products a_i * b_j, i + j = k
+            j = k - i
+            x = p.reg()
+            p.mac(x, a[i], b[j], 4)               # a_i * 4 + b_j
+            lo = p.reg()
+            p.pbs(lo, x, "MultCarryMsgLsb")
+            cols[k].append(lo)
+            if k + 1 < BLOCKS:
+                hi = p.reg()
+                p.pbs(hi, x, "MultCarryMsgMsb")
+                cols[k + 1].append(hi)
+            p.release(x)
+        terms = cols[k]
+        while len(terms) > 1:                     # carry-save: <= 5 terms of <= 3 sum to <= 15
+            grp, terms = terms[:5], terms[5:]
+            s = grp[0]
+            for t in grp[1:]:
+                p.add(s, s, t)
+                p.release(t)
+            m = p.reg()
+            p.pbs(m, s, "MsgOnly")
+            if k + 1 < BLOCKS:
+                c = p.reg()
+                p.pbs(c, s, "CarryInMsg")
+                cols[k + 1].append(c)
+            p.release(s)
+            terms.append(m)
+        p.st(k, terms[0])
+        p.release(terms[0])
+    return p.array()
+
+
+# ------------------------------------------------------ plaintext reference
+
+def run_plain(words, src, n_dst):
+    """Execute a DOp program on clear payloads (the 5-bit padded space) with
+    the LUT semantics of a PBS; asserts that every PBS input stays below 16."""
+    regs = [0] * 128
+    dst = [0] * n_dst
+    tables = lut_tables()
+    for w in (int(x) for x in words):
+        op = w >> 26
+        d, s0, s1 = w & 0x7F, (w >> 7) & 0x7F, (w >> 14) & 0x7F
+        if op == OPC["LD"]:
+            regs[d] = src[(w >> 10) & 0xFFFF] % 32
+        elif op == OPC["ST"]:
+            dst[(w >> 10) & 0xFFFF] = regs[d]
+        elif op == OPC["ADD"]:
+            regs[d] = (regs[s0] + regs[s1]) % 32
+        elif op == OPC["SUB"]:
+            regs[d] = (regs[s0] - regs[s1]) % 32
+        elif op == OPC["MAC"]:
+            regs[d] = (regs[s0] * ((w >> 21) & 0x1F) + regs[s1]) % 32
+        elif op in (OPC["PBS"], OPC["PBS_ML2"], OPC["PBS_ML4"], OPC["PBS_ML8"]):
+            k = 1 << (op - OPC["PBS"])
+            x = regs[s0]
+            assert x < 16 // k, f"PBS input {x} out of range for {k} functions"
+            t = tables[(w >> 14) & 0xFFF]
+            for m in range(k):
+                regs[d + m] = t[m * (16 // k) + x]
+        elif op == OPC["SYNC"]:
+            pass
+        else:
+            raise ValueError(f"opcode 0x{op:02x} not modelled")
+    return dst
+
+
+def to_blocks(v):
+    return [(v >> (2 * i)) & 3 for i in range(BLOCKS)]
+
+
+def from_blocks(bs):
+    return sum((int(b) & 3) << (2 * i) for i, b in enumerate(bs))

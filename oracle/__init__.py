@@ -55,6 +55,7 @@ def lib():
         L.or_bsk_free.argtypes = [vp]
         L.or_blind_rotate.argtypes = [vp, vp, vp, vp, vp, u32, u32]
         L.or_ks_pbs.argtypes = [vp, vp, vp, vp, vp, vp, u32, u32, u32, u32, u32]
+        L.or_ks_pbs_ml.argtypes = [vp, vp, vp, vp, vp, vp, u32, u32, u32, u32, u32, u32]
         L.or_num_threads.restype = ctypes.c_int
         L.or_set_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -149,14 +150,15 @@ class OracleBsk:
         lib().or_blind_rotate(self.h, _p(lwe2N), _p(luts), _p(lut_ids), _p(out), lwe2N.shape[0], pbs_bl)
         return out
 
-    def ks_pbs(self, ksk, blwe_in, luts, lut_ids, ks_bl=3, ks_lc=6, ks_w=21, pbs_bl=23):
+    def ks_pbs(self, ksk, blwe_in, luts, lut_ids, ks_bl=3, ks_lc=6, ks_w=21, pbs_bl=23, mlk=1):
+        """KS+PBS; with mlk > 1 (many-LUT) row c*mlk+m holds output m of input c."""
         ksk = np.ascontiguousarray(ksk, np.uint32)
         blwe_in = np.ascontiguousarray(blwe_in, np.uint64).reshape(-1, self.N + 1)
         luts = np.ascontiguousarray(luts, np.uint64)
         lut_ids = np.ascontiguousarray(lut_ids, np.uint32)
-        out = np.zeros_like(blwe_in)
-        lib().or_ks_pbs(self.h, _p(ksk), _p(blwe_in), _p(luts), _p(lut_ids), _p(out), blwe_in.shape[0], ks_bl,
-                        ks_lc, ks_w, pbs_bl)
+        out = np.zeros((blwe_in.shape[0] * mlk, self.N + 1), np.uint64)
+        lib().or_ks_pbs_ml(self.h, _p(ksk), _p(blwe_in), _p(luts), _p(lut_ids), _p(out), blwe_in.shape[0], ks_bl,
+                           ks_lc, ks_w, pbs_bl, mlk)
         return out
 
 

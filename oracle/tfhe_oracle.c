@@ -371,7 +371,7 @@ void or_bsk_free(void *h)
 /* One blind rotation + sample extract.  lwe2N: n masks then the body, in [0,2N).
  * lut: GLWE (mask poly, body poly).  out: BLWE, N mask coefs then body. */
 static void br_one(const or_bsk_t *k, const uint32_t *lwe2N, const uint64_t *lut,
-                   uint32_t pbs_bl, uint64_t *out, uint64_t *work)
+                   uint32_t pbs_bl, uint64_t *out, uint64_t *work, uint32_t mlk)
 {
     uint32_t N = k->N, n = k->n;
     uint64_t *acc = work, *rot = work + 2 * N, *dh = work + 4 * N, *rh = work + 6 * N;
@@ -400,18 +400,22 @@ static void br_one(const or_bsk_t *k, const uint32_t *lwe2N, const uint64_t *lut
             for (uint32_t j = 0; j < N; j++) acc[col * N + j] += or_modsw_p_to_q(rh[col * N + j]);
         }
     }
-    /* sample extract of coefficient 0 of X^{-b} ACC */
-    uint32_t b = lwe2N[n];
-    or_monomial(acc, 2 * N - b, rot, N);
-    or_monomial(acc + N, 2 * N - b, rot + N, N);
-    out[0] = rot[0];
-    for (uint32_t j = 1; j < N; j++) out[j] = (uint64_t)0 - rot[N - j];
-    out[N] = rot[N];
+    /* sample extract of coefficient 0 of X^{-b} ACC; many-LUT output m takes
+     * coefficient m N/mlk instead (docs/dop.md:113-121) */
+    for (uint32_t m = 0; m < mlk; m++) {
+        uint32_t b = (lwe2N[n] + m * (N / mlk)) % (2 * N);
+        uint64_t *o = out + (size_t)m * (N + 1);
+        or_monomial(acc, 2 * N - b, rot, N);
+        or_monomial(acc + N, 2 * N - b, rot + N, N);
+        o[0] = rot[0];
+        for (uint32_t j = 1; j < N; j++) o[j] = (uint64_t)0 - rot[N - j];
+        o[N] = rot[N];
+    }
 }
 
 /* Blind rotation of `B` already key-switched ciphertexts. */
-void or_blind_rotate(void *bsk, const uint32_t *lwe2N, const uint64_t *luts, const uint32_t *lut_id,
-                     uint64_t *out, uint32_t B, uint32_t pbs_bl)
+void or_blind_rotate_ml(void *bsk, const uint32_t *lwe2N, const uint64_t *luts, const uint32_t *lut_id,
+                        uint64_t *out, uint32_t B, uint32_t pbs_bl, uint32_t mlk)
 {
     or_bsk_t *k = bsk;
     uint32_t N = k->N, n = k->n;
@@ -421,15 +425,20 @@ void or_blind_rotate(void *bsk, const uint32_t *lwe2N, const uint64_t *luts, con
 #pragma omp for schedule(dynamic, 1)
         for (long c = 0; c < (long)B; c++)
             br_one(k, lwe2N + (size_t)c * (n + 1), luts + (size_t)lut_id[c] * 2 * N, pbs_bl,
-                   out + (size_t)c * (N + 1), work);
+                   out + (size_t)c * mlk * (N + 1), work, mlk);
         free(work);
     }
 }
+void or_blind_rotate(void *bsk, const uint32_t *lwe2N, const uint64_t *luts, const uint32_t *lut_id,
+                     uint64_t *out, uint32_t B, uint32_t pbs_bl)
+{
+    or_blind_rotate_ml(bsk, lwe2N, luts, lut_id, out, B, pbs_bl, 1);
+}
 
 /* Full KS+PBS of B ciphertexts (the PBS DOp: docs/dop.md:101-111). */
-void or_ks_pbs(void *bsk, const uint32_t *ksk, const uint64_t *blwe_in, const uint64_t *luts,
-               const uint32_t *lut_id, uint64_t *blwe_out, uint32_t B, uint32_t ks_bl, uint32_t ks_lc,
-               uint32_t ks_w, uint32_t pbs_bl)
+void or_ks_pbs_ml(void *bsk, const uint32_t *ksk, const uint64_t *blwe_in, const uint64_t *luts,
+                  const uint32_t *lut_id, uint64_t *blwe_out, uint32_t B, uint32_t ks_bl, uint32_t ks_lc,
+                  uint32_t ks_w, uint32_t pbs_bl, uint32_t mlk)
 {
     or_bsk_t *k = bsk;
     uint32_t N = k->N, n = k->n;
@@ -443,8 +452,14 @@ void or_ks_pbs(void *bsk, const uint32_t *ksk, const uint64_t *blwe_in, const ui
                          l2n + (size_t)c * (n + 1));
         free(o21);
     }
-    or_blind_rotate(bsk, l2n, luts, lut_id, blwe_out, B, pbs_bl);
+    or_blind_rotate_ml(bsk, l2n, luts, lut_id, blwe_out, B, pbs_bl, mlk);
     free(l2n);
+}
+void or_ks_pbs(void *bsk, const uint32_t *ksk, const uint64_t *blwe_in, const uint64_t *luts,
+               const uint32_t *lut_id, uint64_t *blwe_out, uint32_t B, uint32_t ks_bl, uint32_t ks_lc,
+               uint32_t ks_w, uint32_t pbs_bl)
+{
+    or_ks_pbs_ml(bsk, ksk, blwe_in, luts, lut_id, blwe_out, B, ks_bl, ks_lc, ks_w, pbs_bl, 1);
 }
 
 int or_num_threads(void)

@@ -1,0 +1,161 @@
+"""Many-LUT PBS and the serving loop on the GPU: bit-exact against the CPU
+oracle, decrypting to the right integers, and identical alone and in a mix."""
+import numpy as np
+import pytest
+
+import luthe_b200 as L
+import oracle
+from luthe_b200 import iops as I
+from conftest import from_dev, to_dev
+
+pytestmark = pytest.mark.gpu
+N = 2048
+
+
+@pytest.fixture(scope="module")
+def iop_luts(params):
+    return np.stack([L.lut_build(params, t) for t in I.lut_tables()])
+
+
+def enc_blocks(params, keys, values, seed):
+    blocks = [b for v in values for b in I.to_blocks(v)]
+    return L.encrypt(params, keys["glwe_key"], np.array(blocks, np.uint32), seed)
+
+
+def dec_blocks(params, keys, blwe):
+    return [int(x) for x in L.decrypt(params, keys["glwe_key"], blwe)]
+
+
+@pytest.mark.parametrize("mlk", [2, 4])
+def test_many_lut_matches_oracle(engine, params, keys, oracle_bsk, mlk):
+    rng = np.random.default_rng(100 + mlk)
+    span = 16 // mlk
+    fs = [rng.integers(0, 16, span).astype(np.uint32) for _ in range(mlk)]
+    table = np.concatenate(fs)
+    luts = L.lut_build(params, table)[None]
+    msgs = rng.integers(0, span, 5).astype(np.uint32)
+    ct = L.encrypt(params, keys["glwe_key"], msgs, 300 + mlk)
+    engine.upload_luts(luts)
+    ids = np.zeros(5, np.uint32)
+    d_out = to_dev(np.zeros((5 * mlk, N + 1), np.uint64))
+    engine.ks_pbs_ml(to_dev(ct), to_dev(ids), d_out, 5, mlk)
+    engine.check_device_error()
+    got = from_dev(d_out, np.uint64)
+    want = oracle_bsk.ks_pbs(keys["ksk"], ct, luts, ids, mlk=mlk)
+    assert np.array_equal(got, want)
+    dec = dec_blocks(params, keys, got)
+    assert dec == [int(fs[m][x]) for x in msgs for m in range(mlk)]
+
+
+def oracle_run(program, src, n_dst, keys, oracle_bsk, luts):
+    """Execute a DOp program on ciphertexts with the CPU oracle (PBS runs of
+    mutually independent PBS DOps are batched)."""
+    regs = {}
+    dst = [None] * n_dst
+    words = [int(w) for w in program]
+    i = 0
+    while i < len(words):
+        w = words[i]
+        op, d, s0, s1 = w >> 26, w & 0x7F, (w >> 7) & 0x7F, (w >> 14) & 0x7F
+        if op >= 0x30:
+            batch, written = [], set()
+            while i < len(words) and (words[i] >> 26) >= 0x30 and ((words[i] >> 7) & 0x7F) not in written:
+                ww = words[i]
+                k = 1 << ((ww >> 26) - 0x30)
+                batch.append(ww)
+                written.update(range(ww & 0x7F, (ww & 0x7F) + k))
+                i += 1
+            ks = sorted({1 << ((x >> 26) - 0x30) for x in batch})
+            for k in ks:
+                sub = [x for x in batch if (1 << ((x >> 26) - 0x30)) == k]
+                cts = np.stack([regs[(x >> 7) & 0x7F] for x in sub])
+                gids = np.array([(x >> 14) & 0xFFF for x in sub], np.uint32)
+                out = oracle_bsk.ks_pbs(keys["ksk"], cts, luts, gids, mlk=k)
+                for j, x in enumerate(sub):
+                    for m in range(k):
+                        regs[(x & 0x7F) + m] = out[j * k + m]
+            continue
+        with np.errstate(over="ignore"):
+            if op == 0x20:
+                regs[d] = src[(w >> 10) & 0xFFFF].copy()
+            elif op == 0x21:
+                dst[(w >> 10) & 0xFFFF] = regs[d].copy()
+            elif op == 0x01:
+                regs[d] = regs[s0] + regs[s1]
+            elif op == 0x05:
+                regs[d] = regs[s0] * np.uint64((w >> 21) & 0x1F) + regs[s1]
+            else:
+                raise ValueError(hex(op))
+        i += 1
+    return np.stack(dst)
+
+
+def test_serving_add_and_cmp_bit_exact_vs_oracle(engine, params, keys, oracle_bsk, iop_luts):
+    engine.upload_luts(iop_luts)
+    srv = L.Server(engine, pool_bytes=256 << 20)
+    a, b, k = 0xBEEF, 0x1357, 0x4000
+    reqs = [(I.prog_add(), enc_blocks(params, keys, [a, b], 11), 8),
+            (I.prog_cmp_gt(k), enc_blocks(params, keys, [a], 12), 1)]
+    outs = srv.run(reqs)
+    srv.close()
+    assert I.from_blocks(dec_blocks(params, keys, outs[0])) == (a + b) % 65536
+    assert dec_blocks(params, keys, outs[1]) == [int(a > k)]
+    for (prog, src, nd), got in zip(reqs, outs):
+        assert np.array_equal(got, oracle_run(prog, src, nd, keys, oracle_bsk, iop_luts))
+
+
+def test_serving_mix_equals_alone(engine, params, keys, iop_luts):
+    engine.upload_luts(iop_luts)
+    rng = np.random.default_rng(5)
+    reqs, expect = [], []
+    for r in range(9):
+        a, b = int(rng.integers(65536)), int(rng.integers(65536))
+        kind = r % 3
+        if kind == 0:
+            reqs.append((I.prog_add(), enc_blocks(params, keys, [a, b], 50 + r), 8))
+            expect.append((a + b) % 65536)
+        elif kind == 1:
+            reqs.append((I.prog_cmp_gt(b), enc_blocks(params, keys, [a], 50 + r), 1))
+            expect.append(int(a > b))
+        else:
+            reqs.append((I.prog_mul(), enc_blocks(params, keys, [a, b], 50 + r), 8))
+            expect.append((a * b) % 65536)
+    srv = L.Server(engine, pool_bytes=512 << 20)
+    mixed = srv.run(reqs)
+    alone = [srv.run([r])[0] for r in reqs[:3]]      # one of each kind on its own
+    counters = srv.counters()
+    srv.close()
+    for got, want, (prog, _, nd) in zip(mixed, expect, reqs):
+        dec = dec_blocks(params, keys, got)
+        assert (I.from_blocks(dec) if nd == 8 else dec[0]) == want
+    for m, s in zip(mixed[:3], alone):
+        assert np.array_equal(m, s)
+    assert counters["pbs"] == 3 * (8 + 16 + 101) + 8 + 16 + 101
+
+
+def test_serving_admission_is_bounded_by_the_pool(engine, params, keys, iop_luts):
+    engine.upload_luts(iop_luts)
+    slot = (N + 1) * 8
+    srv = L.Server(engine, pool_bytes=310 * slot)      # an ADD request takes 152 slots: room for 2
+    reqs = [(I.prog_add(), enc_blocks(params, keys, [i, 2 * i], 70 + i), 8) for i in range(5)]
+    ids = [srv.submit(*r) for r in reqs]
+    done, max_active = 0, 0
+    while done < len(ids):
+        c, active, pending = srv.step()
+        max_active = max(max_active, active + c)
+        done += c
+    assert max_active <= 2
+    for i, rid in enumerate(ids):
+        out, lat, q = srv.fetch(rid, 8)
+        assert I.from_blocks(dec_blocks(params, keys, out)) == 3 * i
+    srv.close()
+
+
+def test_serving_rejects_bad_programs(engine, iop_luts):
+    engine.upload_luts(iop_luts)
+    srv = L.Server(engine, pool_bytes=64 << 20)
+    with pytest.raises(L.LutheError):
+        srv.submit(np.array([I.enc_pbs("PBS", 0, 1, 4000)], np.uint32), np.zeros((0, N + 1), np.uint64), 1)
+    with pytest.raises(L.LutheError):
+        srv.submit(np.array([I.enc_mem("LD", 0, I.MEM_SRC, 5)], np.uint32), np.zeros((1, N + 1), np.uint64), 1)
+    srv.close()

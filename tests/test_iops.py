@@ -1,0 +1,58 @@
+"""DOp programs of the radix IOps (no GPU): plaintext semantics, encodings and
+register use."""
+import random
+
+import numpy as np
+import pytest
+
+from luthe_b200 import iops as I
+
+EDGE = [0, 1, 3, 4, 255, 256, 0x5555, 0xAAAA, 0x7FFF, 0x8000, 0xFFFE, 0xFFFF]
+
+
+@pytest.mark.parametrize("a,b", [(x, y) for x in EDGE for y in EDGE[::3]])
+def test_add_and_mul_edges(a, b):
+    src = I.to_blocks(a) + I.to_blocks(b)
+    assert I.from_blocks(I.run_plain(I.prog_add(), src, 8)) == (a + b) % 65536
+    assert I.from_blocks(I.run_plain(I.prog_mul(), src, 8)) == (a * b) % 65536
+
+
+@pytest.mark.parametrize("a,k", [(x, y) for x in EDGE for y in EDGE[::2]])
+def test_cmp_edges(a, k):
+    assert I.run_plain(I.prog_cmp_gt(k), I.to_blocks(a), 1) == [int(a > k)]
+
+
+def test_random_programs():
+    rng = random.Random(7)
+    for _ in range(200):
+        a, b, k = rng.randrange(65536), rng.randrange(65536), rng.randrange(65536)
+        src = I.to_blocks(a) + I.to_blocks(b)
+        assert I.from_blocks(I.run_plain(I.prog_add(), src, 8)) == (a + b) % 65536
+        assert I.from_blocks(I.run_plain(I.prog_mul(), src, 8)) == (a * b) % 65536
+        assert I.run_plain(I.prog_cmp_gt(k), I.to_blocks(a), 1) == [int(a > k)]
+
+
+def test_dop_field_layout():
+    # fields LSB first (fw/ublaze/src/hpu_dop_fmt.h:56-99)
+    w = I.enc_pbs("PBS_ML2", 6, 9, 5)
+    assert w >> 26 == 0x31 and (w >> 14) & 0xFFF == 5 and (w >> 7) & 0x7F == 9 and w & 0x7F == 6
+    assert (w >> 26) >> 4 == 0b11                      # kind PBS
+    w = I.enc_arith("MAC", 1, 2, 3, 4)
+    assert w >> 26 == 0x05 and (w >> 21) & 0x1F == 4 and (w >> 14) & 0x7F == 3
+    assert (w >> 26) & 0b0100 and (w >> 26) & 0b0001   # MUL | ADD flags
+    w = I.enc_mem("LD", 7, I.MEM_SRC, 300)
+    assert (w >> 26) >> 4 == 0b10 and (w >> 10) & 0xFFFF == 300 and (w >> 8) & 3 == 2
+
+
+def test_programs_fit_the_register_file():
+    for prog in (I.prog_add(), I.prog_cmp_gt(0x1234), I.prog_mul()):
+        for w in prog:
+            w = int(w)
+            assert w & 0x7F < 128
+        assert len(prog) < 4096
+
+
+def test_many_lut_table_layout():
+    t = I.LUTS["ManyCarryMsg"]
+    for x in range(8):
+        assert t[x] == x & 3 and t[8 + x] == x >> 2
