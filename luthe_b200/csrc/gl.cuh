@@ -113,11 +113,44 @@ __device__ __forceinline__ u64 shl(u64 x)
         return neg(shl<s - 96>(x));  // 2^96 == -1
     } else if constexpr (s <= 32) {
         return reduce96(x << s, (u32)(x >> (64 - s)));
-    } else if constexpr (s < 64) {
-        return reduce128(x << s, x >> (64 - s));
     } else {
-        return shl<32>(shl<s - 32>(x));
+        return shl<32>(shl<s - 32>(x));  // two 96-bit folds beat one 128-bit fold
     }
+}
+
+// x * 2^s for a runtime s in [0, 192) that is uniform across the warp: one
+// copy of the code serves every exponent (the pass twiddles), the branches
+// never diverge.
+__device__ __forceinline__ u64 shl_rt(u64 x, u32 s)
+{
+    const bool negate = s >= 96;
+    if (negate) s -= 96;
+    if (s > 32) {
+        const u32 s1 = s > 64 ? 32 : s - 32;  // first fold: s1 in [1, 32]
+        x = reduce96(x << s1, (u32)(x >> (64 - s1)));
+        s -= s1;
+        if (s > 32) {
+            x = reduce96(x << 32, (u32)(x >> 32));
+            s -= 32;
+        }
+    }
+    if (s) x = reduce96(x << s, (u32)(x >> (64 - s)));
+    return negate ? neg(x) : x;
+}
+
+// a*b + c*d with one reduction: the two 128-bit products are summed first;
+// a carry out of bit 128 is worth 2^128 == -2^32 (mod p).
+__device__ __forceinline__ u64 mul_add2(u64 a, u64 b, u64 c, u64 d)
+{
+    u64 lo, hi;
+    u32 c2;
+    const u64 l1 = a * b, h1 = __umul64hi(a, b), l2 = c * d, h2 = __umul64hi(c, d);
+    asm("add.cc.u64 %0, %3, %4;\n\t"
+        "addc.cc.u64 %1, %5, %6;\n\t"
+        "addc.u32 %2, 0, 0;"
+        : "=l"(lo), "=l"(hi), "=r"(c2)
+        : "l"(l1), "l"(l2), "l"(h1), "l"(h2));
+    return sub(reduce128(lo, hi), (u64)c2 << 32);
 }
 
 // Cooley-Tukey butterfly: (u, v) <- (u + v 2^S, u - v 2^S)

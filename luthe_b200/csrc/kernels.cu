@@ -458,8 +458,8 @@ __global__ void __launch_bounds__(G * 256, 1)
             for (int p = 0; p < 8; p++) {
                 const u64 *sb = slab + p * 4 * TPG + t;
                 const u64 b00 = sb[0], b01 = sb[TPG], b10 = sb[2 * TPG], b11 = sb[3 * TPG];
-                r[0][p] = gl::add(gl::mul(x[0][p], b00), gl::mul(x[1][p], b10));
-                r[1][p] = gl::add(gl::mul(x[0][p], b01), gl::mul(x[1][p], b11));
+                r[0][p] = gl::mul_add2(x[0][p], b00, x[1][p], b10);
+                r[1][p] = gl::mul_add2(x[0][p], b01, x[1][p], b11);
             }
             if (__syncthreads_or(!ok)) {
                 if (threadIdx.x == 0) atomicExch(err, 1u);

@@ -141,14 +141,16 @@ __device__ __forceinline__ void tw_a1(u64 *y)
     y[6] = gl::shl<SIGN * 3 * J1A * (2 * brv3(6) + 1)>(y[6]);
     y[7] = gl::shl<SIGN * 3 * J1A * (2 * brv3(7) + 1)>(y[7]);
 }
+// Runtime forms: one copy of the shift code for every warp-uniform j1a / j2a
+// (the templated forms above, one per value, overflow the instruction cache).
 template <int SIGN>
 __device__ __forceinline__ void tw_a1_rt(u64 *y, int j1a)
 {
-    switch (j1a) {
-    case 1: tw_a1<1, SIGN>(y); break;
-    case 2: tw_a1<2, SIGN>(y); break;
-    case 3: tw_a1<3, SIGN>(y); break;
-    default: break;
+    if (j1a == 0) return;
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        const u32 e = 3u * j1a * (2 * brv3(p) + 1);  // < 192
+        y[p] = gl::shl_rt(y[p], SIGN > 0 ? e : (192u - e) % 192u);
     }
 }
 template <int J2A, int SIGN>
@@ -166,15 +168,11 @@ __device__ __forceinline__ void tw_c1(u64 *y)
 template <int SIGN>
 __device__ __forceinline__ void tw_c1_rt(u64 *y, int j2a)
 {
-    switch (j2a) {
-    case 1: tw_c1<1, SIGN>(y); break;
-    case 2: tw_c1<2, SIGN>(y); break;
-    case 3: tw_c1<3, SIGN>(y); break;
-    case 4: tw_c1<4, SIGN>(y); break;
-    case 5: tw_c1<5, SIGN>(y); break;
-    case 6: tw_c1<6, SIGN>(y); break;
-    case 7: tw_c1<7, SIGN>(y); break;
-    default: break;
+    if (j2a == 0) return;
+#pragma unroll
+    for (int p = 1; p < 8; p++) {  // p = 0 has k2b = 0: twiddle 1
+        const u32 e = 3u * j2a * brv3(p);  // < 192
+        y[p] = gl::shl_rt(y[p], SIGN > 0 ? e : (192u - e) % 192u);
     }
 }
 
