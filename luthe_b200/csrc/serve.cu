@@ -21,6 +21,7 @@
 #include <deque>
 #include <map>
 #include <string.h>
+#include <thread>
 #include <vector>
 #include "ctx.h"
 
@@ -55,10 +56,11 @@ struct Request {
     uint64_t id;
     std::vector<Instr> prog;
     uint32_t n_src, n_dst, n_heap, n_slots;
-    uint32_t base = 0;         // first pool slot
-    std::vector<uint64_t> h_src, h_dst;
+    uint32_t base = 0;         // first device pool slot
+    uint32_t hbase = 0;        // first pinned host slot: [src][dst]
     std::vector<int> ready;
     size_t remaining = 0;
+    cudaEvent_t retired = nullptr;  // outputs copied back
     clock_t_::time_point t_submit, t_admit, t_done;
 };
 
@@ -188,54 +190,95 @@ void build_dag(Request &r)
     r.remaining = r.prog.size();
 }
 
+// First-fit allocator over slot ranges (device pool and pinned host staging).
+struct SlotPool {
+    std::vector<std::pair<uint32_t, uint32_t>> free_list;  // (start, len), sorted
+    void init(uint32_t n) { free_list.assign(1, {0, n}); }
+    bool alloc(uint32_t len, uint32_t &start)
+    {
+        for (size_t i = 0; i < free_list.size(); i++)
+            if (free_list[i].second >= len) {
+                start = free_list[i].first;
+                free_list[i].first += len;
+                free_list[i].second -= len;
+                if (free_list[i].second == 0) free_list.erase(free_list.begin() + i);
+                return true;
+            }
+        return false;
+    }
+    void release(uint32_t start, uint32_t len)
+    {
+        if (!len) return;
+        auto it = free_list.begin();
+        while (it != free_list.end() && it->first < start) ++it;
+        auto ins = free_list.insert(it, {start, len});  // may reallocate: take begin() after it
+        size_t i = ins - free_list.begin();
+        if (i + 1 < free_list.size() && free_list[i].first + free_list[i].second == free_list[i + 1].first) {
+            free_list[i].second += free_list[i + 1].second;
+            free_list.erase(free_list.begin() + i + 1);
+        }
+        if (i > 0 && free_list[i - 1].first + free_list[i - 1].second == free_list[i].first) {
+            free_list[i - 1].second += free_list[i].second;
+            free_list.erase(free_list.begin() + i);
+        }
+    }
+};
+
+// One PBS lane: a stream with its own KS scratch and index arrays, so that
+// batches issued at different times run concurrently on the GPU.
+struct Lane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    uint32_t *d_l2n = nullptr;   // [max_pbs][n+1]
+    uint32_t *d_idx = nullptr;   // [3][max_pbs]: src, dst, gid
+    uint32_t *h_idx = nullptr;   // pinned staging of d_idx
+    std::vector<std::pair<Request *, int>> ops;
+    bool busy = false;
+};
+
+constexpr int LANES = 6;
+
 }  // namespace
 
 struct luthe_server {
     luthe_ctx *ctx = nullptr;
     uint64_t *d_pool = nullptr;
     uint32_t nslots = 0;
-    std::vector<std::pair<uint32_t, uint32_t>> free_list;  // (start, len), sorted
+    SlotPool dev, host;
+    uint64_t *h_pool = nullptr;  // pinned staging, same slot size
+    uint32_t nhost = 0;
     std::deque<Request *> pending;
-    std::vector<Request *> active;
+    std::vector<Request *> active, retiring;
     std::map<uint64_t, Request *> done;
     uint64_t next_id = 1;
-    cudaStream_t stream = nullptr;
-    AluOp *d_ops = nullptr;
-    uint32_t ops_cap = 0;
-    uint32_t *d_idx = nullptr;  // [src | dst | gid] of a PBS batch
-    uint32_t idx_cap = 0;
+    cudaStream_t alu_stream = nullptr;
+    cudaEvent_t alu_done = nullptr;
+    Lane lanes[LANES];
+    AluOp *d_ops = nullptr, *h_ops = nullptr;  // pinned ring of ALU descriptors
+    uint32_t ops_cap = 0, ops_head = 0;
     uint32_t max_pbs = 4096;
-    uint64_t rounds = 0, pbs_done = 0, alu_done = 0, launches = 0;
+    uint64_t rounds = 0, pbs_done = 0, alu_done_n = 0, launches = 0;
 };
 
-static bool pool_alloc(luthe_server *s, uint32_t len, uint32_t &start)
+namespace {
+
+int check_err(luthe_ctx *c)
 {
-    for (size_t i = 0; i < s->free_list.size(); i++)
-        if (s->free_list[i].second >= len) {
-            start = s->free_list[i].first;
-            s->free_list[i].first += len;
-            s->free_list[i].second -= len;
-            if (s->free_list[i].second == 0) s->free_list.erase(s->free_list.begin() + i);
-            return true;
-        }
-    return false;
+    uint32_t e = 0;
+    CUDA_TRY(cudaMemcpy(&e, c->d_err, 4, cudaMemcpyDeviceToHost));
+    if (e) return fail(LUTHE_E_TIMEOUT, "blind rotation: bounded wait for a BSK slab ran out");
+    return LUTHE_OK;
 }
-static void pool_free(luthe_server *s, uint32_t start, uint32_t len)
+
+void finish(Request *r, int i)
 {
-    auto it = s->free_list.begin();
-    while (it != s->free_list.end() && it->first < start) ++it;
-    it = s->free_list.insert(it, {start, len});
-    // merge with neighbours
-    size_t i = it - s->free_list.begin();
-    if (i + 1 < s->free_list.size() && s->free_list[i].first + s->free_list[i].second == s->free_list[i + 1].first) {
-        s->free_list[i].second += s->free_list[i + 1].second;
-        s->free_list.erase(s->free_list.begin() + i + 1);
-    }
-    if (i > 0 && s->free_list[i - 1].first + s->free_list[i - 1].second == s->free_list[i].first) {
-        s->free_list[i - 1].second += s->free_list[i].second;
-        s->free_list.erase(s->free_list.begin() + i);
-    }
+    r->prog[i].done = true;
+    r->remaining--;
+    for (int j : r->prog[i].succ)
+        if (--r->prog[j].npred == 0) r->ready.push_back(j);
 }
+
+}  // namespace
 
 extern "C" int luthe_server_create(luthe_ctx *c, uint64_t pool_bytes, uint32_t max_pbs, luthe_server **out)
 {
@@ -246,23 +289,35 @@ extern "C" int luthe_server_create(luthe_ctx *c, uint64_t pool_bytes, uint32_t m
     CUDA_TRY(cudaSetDevice(c->device));
     const size_t slot_bytes = (size_t)(c->p.poly_size + 1) * 8;
     const uint64_t nslots = pool_bytes / slot_bytes;
-    if (nslots < 2 * NREG || nslots > 0xFFFFFFFFull) return fail(LUTHE_E_PARAM, "pool of %llu slots is out of range",
-                                                                  (unsigned long long)nslots);
+    if (nslots < 2 * NREG || nslots > 0xFFFFFFFFull)
+        return fail(LUTHE_E_PARAM, "pool of %llu slots is out of range", (unsigned long long)nslots);
     luthe_server *s = new luthe_server();
     s->ctx = c;
     s->nslots = (uint32_t)nslots;
     s->max_pbs = max_pbs ? max_pbs : 4096;
-    if ((r = dalloc(c, (void **)&s->d_pool, nslots * slot_bytes)) || (r = ensure_scratch(c, s->max_pbs)) ||
-        (r = dalloc(c, (void **)&s->d_idx, (size_t)s->max_pbs * 3 * 4))) {
-        luthe_server_destroy(s);
-        return r;
+    s->nhost = (uint32_t)std::min<uint64_t>(nslots, 65536);
+    s->ops_cap = 1u << 16;
+    const size_t n1 = c->p.lwe_dim + 1;
+    bool ok = !dalloc(c, (void **)&s->d_pool, nslots * slot_bytes) &&
+              !dalloc(c, (void **)&s->d_ops, (size_t)s->ops_cap * sizeof(AluOp)) &&
+              cudaMallocHost((void **)&s->h_pool, (size_t)s->nhost * slot_bytes) == cudaSuccess &&
+              cudaMallocHost((void **)&s->h_ops, (size_t)s->ops_cap * sizeof(AluOp)) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s->alu_stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&s->alu_done, cudaEventDisableTiming) == cudaSuccess;
+    for (int l = 0; ok && l < LANES; l++) {
+        Lane &ln = s->lanes[l];
+        ok = !dalloc(c, (void **)&ln.d_l2n, (size_t)s->max_pbs * n1 * 4) &&
+             !dalloc(c, (void **)&ln.d_idx, (size_t)s->max_pbs * 3 * 4) &&
+             cudaMallocHost((void **)&ln.h_idx, (size_t)s->max_pbs * 3 * 4) == cudaSuccess &&
+             cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&ln.done, cudaEventDisableTiming) == cudaSuccess;
     }
-    s->idx_cap = s->max_pbs;
-    s->free_list.push_back({0, s->nslots});
-    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (!ok) {
         luthe_server_destroy(s);
-        return fail(LUTHE_E_CUDA, "stream creation failed");
+        return fail(LUTHE_E_BUDGET, "server resources could not be allocated (%s)", g_err);
     }
+    s->dev.init(s->nslots);
+    s->host.init(s->nhost);
     *out = s;
     return LUTHE_OK;
 }
@@ -272,16 +327,29 @@ extern "C" void luthe_server_destroy(luthe_server *s)
     if (!s) return;
     luthe_ctx *c = s->ctx;
     cudaSetDevice(c->device);
-    if (s->stream) {
-        cudaStreamSynchronize(s->stream);
-        cudaStreamDestroy(s->stream);
+    const size_t n1 = c->p.lwe_dim + 1;
+    cudaDeviceSynchronize();
+    for (Lane &ln : s->lanes) {
+        if (ln.stream) cudaStreamDestroy(ln.stream);
+        if (ln.done) cudaEventDestroy(ln.done);
+        if (ln.h_idx) cudaFreeHost(ln.h_idx);
+        dfree(c, ln.d_l2n, ln.d_l2n ? (size_t)s->max_pbs * n1 * 4 : 0);
+        dfree(c, ln.d_idx, ln.d_idx ? (size_t)s->max_pbs * 3 * 4 : 0);
     }
-    dfree(c, s->d_pool, (size_t)s->nslots * (c->p.poly_size + 1) * 8);
-    dfree(c, s->d_ops, (size_t)s->ops_cap * sizeof(AluOp));
-    dfree(c, s->d_idx, (size_t)s->idx_cap * 3 * 4);
-    for (auto *r : s->pending) delete r;
-    for (auto *r : s->active) delete r;
-    for (auto &kv : s->done) delete kv.second;
+    if (s->alu_stream) cudaStreamDestroy(s->alu_stream);
+    if (s->alu_done) cudaEventDestroy(s->alu_done);
+    if (s->h_pool) cudaFreeHost(s->h_pool);
+    if (s->h_ops) cudaFreeHost(s->h_ops);
+    dfree(c, s->d_pool, s->d_pool ? (size_t)s->nslots * (c->p.poly_size + 1) * 8 : 0);
+    dfree(c, s->d_ops, s->d_ops ? (size_t)s->ops_cap * sizeof(AluOp) : 0);
+    auto drop = [](Request *r) {
+        if (r->retired) cudaEventDestroy(r->retired);
+        delete r;
+    };
+    for (auto *r : s->pending) drop(r);
+    for (auto *r : s->active) drop(r);
+    for (auto *r : s->retiring) drop(r);
+    for (auto &kv : s->done) drop(kv.second);
     delete s;
 }
 
@@ -303,9 +371,12 @@ extern "C" int luthe_server_submit(luthe_server *s, const uint32_t *dops, uint32
         delete r;
         return fail(LUTHE_E_BUDGET, "request needs %u slots, the pool has %u", r->n_slots, s->nslots);
     }
+    if (!s->host.alloc(n_src + n_dst, r->hbase)) {
+        delete r;
+        return fail(LUTHE_E_BUDGET, "pinned staging full: retire finished requests first");
+    }
     const size_t w = s->ctx->p.poly_size + 1;
-    r->h_src.assign(h_src, h_src + (size_t)n_src * w);
-    r->h_dst.assign((size_t)n_dst * w, 0);
+    memcpy(s->h_pool + (size_t)r->hbase * w, h_src, (size_t)n_src * w * 8);
     r->id = s->next_id++;
     r->t_submit = clock_t_::now();
     s->pending.push_back(r);
@@ -313,7 +384,8 @@ extern "C" int luthe_server_submit(luthe_server *s, const uint32_t *dops, uint32
     return LUTHE_OK;
 }
 
-// one scheduling round: admit, linear waves, one PBS batch, retire
+// One pass of the asynchronous scheduler: harvest finished PBS lanes and
+// retirements, admit, issue ready linear DOps, issue ready PBS on idle lanes.
 extern "C" int luthe_server_step(luthe_server *s, uint32_t *n_completed, uint32_t *n_active, uint32_t *n_pending)
 {
     if (!s) return fail(LUTHE_E_PARAM, "null server");
@@ -322,30 +394,57 @@ extern "C" int luthe_server_step(luthe_server *s, uint32_t *n_completed, uint32_
     const size_t w = c->p.poly_size + 1;
     const uint32_t n = c->p.lwe_dim;
     uint32_t completed = 0;
+    bool progress = false;
 
-    // admission: FIFO while the pool has room
+    // PBS lanes whose batch finished: their DOps are done
+    for (Lane &ln : s->lanes) {
+        if (!ln.busy) continue;
+        cudaError_t q = cudaEventQuery(ln.done);
+        if (q == cudaErrorNotReady) continue;
+        CUDA_TRY(q);
+        for (auto &p : ln.ops) finish(p.first, p.second);
+        ln.ops.clear();
+        ln.busy = false;
+        progress = true;
+        int r = check_err(c);
+        if (r) return r;
+    }
+    // requests whose outputs reached the pinned staging
+    for (size_t i = 0; i < s->retiring.size();) {
+        Request *r = s->retiring[i];
+        cudaError_t q = cudaEventQuery(r->retired);
+        if (q == cudaErrorNotReady) {
+            i++;
+            continue;
+        }
+        CUDA_TRY(q);
+        r->t_done = clock_t_::now();
+        cudaEventDestroy(r->retired);
+        r->retired = nullptr;
+        s->dev.release(r->base, r->n_slots);
+        s->done[r->id] = r;
+        s->retiring.erase(s->retiring.begin() + i);
+        completed++;
+        progress = true;
+    }
+    // admission: FIFO while the device pool has room
     while (!s->pending.empty()) {
         Request *r = s->pending.front();
         uint32_t base;
-        if (!pool_alloc(s, r->n_slots, base)) break;
+        if (!s->dev.alloc(r->n_slots, base)) break;
         s->pending.pop_front();
         r->base = base;
         r->t_admit = clock_t_::now();
         if (r->n_src)
-            CUDA_TRY(cudaMemcpyAsync(s->d_pool + (size_t)(base + NREG) * w, r->h_src.data(), r->h_src.size() * 8,
-                                     cudaMemcpyHostToDevice, s->stream));
+            CUDA_TRY(cudaMemcpyAsync(s->d_pool + (size_t)(base + NREG) * w, s->h_pool + (size_t)r->hbase * w,
+                                     (size_t)r->n_src * w * 8, cudaMemcpyHostToDevice, s->alu_stream));
         build_dag(*r);
         s->active.push_back(r);
+        progress = true;
     }
-
-    auto finish = [&](Request *r, int i) {
-        r->prog[i].done = true;
-        r->remaining--;
-        for (int j : r->prog[i].succ)
-            if (--r->prog[j].npred == 0) r->ready.push_back(j);
-    };
-
-    // linear DOps, LD/ST copies and SYNCs: waves until none is ready
+    // linear DOps, LD/ST copies and SYNCs, in waves on the ALU stream; they are
+    // stream-ordered, and PBS lanes wait on the ALU stream before reading
+    bool alu_issued = false;
     for (;;) {
         std::vector<AluOp> ops;
         std::vector<std::pair<Request *, int>> issued;
@@ -353,78 +452,39 @@ extern "C" int luthe_server_step(luthe_server *s, uint32_t *n_completed, uint32_
             std::vector<int> keep;
             for (int i : r->ready) {
                 Instr &in = r->prog[i];
-                if (in.kind == 1) {
+                if (in.kind == 1 || (in.kind == 0 && ops.size() >= s->ops_cap / 2)) {
                     keep.push_back(i);
-                } else if (in.kind == 2) {
-                    issued.push_back({r, i});
-                } else {
-                    ops.push_back(AluOp{in.alu_op, r->base + in.dst, r->base + in.a, r->base + in.b, in.imm});
-                    issued.push_back({r, i});
+                    continue;
                 }
+                if (in.kind == 0) ops.push_back(AluOp{in.alu_op, r->base + in.dst, r->base + in.a, r->base + in.b, in.imm});
+                issued.push_back({r, i});
             }
             r->ready.swap(keep);
         }
         if (issued.empty()) break;
         if (!ops.empty()) {
-            if (ops.size() > s->ops_cap) {
-                dfree(c, s->d_ops, (size_t)s->ops_cap * sizeof(AluOp));
-                s->d_ops = nullptr;
-                s->ops_cap = 0;
-                uint32_t cap = (uint32_t)ops.size() * 2;
-                int r = dalloc(c, (void **)&s->d_ops, (size_t)cap * sizeof(AluOp));
-                if (r) return r;
-                s->ops_cap = cap;
+            // descriptors go through a pinned ring; before the ring wraps, the
+            // copies still reading its start must have finished
+            uint32_t head = s->ops_head;
+            if (head + ops.size() > s->ops_cap) {
+                CUDA_TRY(cudaStreamSynchronize(s->alu_stream));
+                head = 0;
             }
-            CUDA_TRY(cudaMemcpyAsync(s->d_ops, ops.data(), ops.size() * sizeof(AluOp), cudaMemcpyHostToDevice,
-                                     s->stream));
-            CUDA_TRY(launch_alu_batch(s->d_ops, s->d_pool, (uint32_t)ops.size(), c->p.poly_size, s->stream));
+            memcpy(s->h_ops + head, ops.data(), ops.size() * sizeof(AluOp));
+            CUDA_TRY(cudaMemcpyAsync(s->d_ops + head, s->h_ops + head, ops.size() * sizeof(AluOp),
+                                     cudaMemcpyHostToDevice, s->alu_stream));
+            CUDA_TRY(launch_alu_batch(s->d_ops + head, s->d_pool, (uint32_t)ops.size(), c->p.poly_size,
+                                      s->alu_stream));
+            s->ops_head = head + (uint32_t)ops.size();
             s->launches++;
-            s->alu_done += ops.size();
+            s->alu_done_n += ops.size();
+            alu_issued = true;
         }
         for (auto &p : issued) finish(p.first, p.second);
+        progress = true;
     }
-
-    // one PBS batch across requests (per many-LUT factor)
-    for (uint32_t mlk : {1u, 2u, 4u, 8u}) {
-        std::vector<uint32_t> src, dst, gid;
-        std::vector<std::pair<Request *, int>> issued;
-        for (Request *r : s->active) {
-            std::vector<int> keep;
-            for (int i : r->ready) {
-                Instr &in = r->prog[i];
-                if (in.kind == 1 && in.mlk == mlk && src.size() < s->max_pbs) {
-                    src.push_back(r->base + in.a);
-                    dst.push_back(r->base + in.dst);
-                    gid.push_back(in.gid);
-                    issued.push_back({r, i});
-                } else {
-                    keep.push_back(i);
-                }
-            }
-            r->ready.swap(keep);
-        }
-        if (issued.empty()) continue;
-        const uint32_t B = (uint32_t)src.size();
-        std::vector<uint32_t> idx(3 * (size_t)B);
-        memcpy(idx.data(), src.data(), B * 4);
-        memcpy(idx.data() + B, dst.data(), B * 4);
-        memcpy(idx.data() + 2 * (size_t)B, gid.data(), B * 4);
-        CUDA_TRY(cudaMemcpyAsync(s->d_idx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, s->stream));
-        CUDA_TRY(launch_keyswitch(s->d_pool, c->d_ksk, nullptr, c->d_lwe2N, B, n, c->xpad, s->stream, s->d_idx));
-        CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, s->d_idx + 2 * (size_t)B, c->nlut, c->d_bsk,
-                                     c->d_tw, s->d_pool, B, n, c->d_err, s->stream, s->d_idx + B, mlk));
-        s->launches += 2;
-        s->pbs_done += B;
-        for (auto &p : issued) finish(p.first, p.second);
-    }
-    s->rounds++;
-
-    CUDA_TRY(cudaStreamSynchronize(s->stream));
-    uint32_t e = 0;
-    CUDA_TRY(cudaMemcpy(&e, c->d_err, 4, cudaMemcpyDeviceToHost));
-    if (e) return fail(LUTHE_E_TIMEOUT, "blind rotation: bounded wait for a BSK slab ran out");
-
-    // retire finished requests
+    if (alu_issued) CUDA_TRY(cudaEventRecord(s->alu_done, s->alu_stream));
+    // finished requests: copy outputs back on the ALU stream
     std::vector<Request *> still;
     for (Request *r : s->active) {
         if (r->remaining) {
@@ -432,20 +492,55 @@ extern "C" int luthe_server_step(luthe_server *s, uint32_t *n_completed, uint32_
             continue;
         }
         if (r->n_dst)
-            CUDA_TRY(cudaMemcpy(r->h_dst.data(), s->d_pool + (size_t)(r->base + NREG + r->n_src) * w,
-                                r->h_dst.size() * 8, cudaMemcpyDeviceToHost));
-        r->t_done = clock_t_::now();
-        pool_free(s, r->base, r->n_slots);
-        r->h_src.clear();
-        r->h_src.shrink_to_fit();
-        r->prog.clear();
-        r->prog.shrink_to_fit();
-        s->done[r->id] = r;
-        completed++;
+            CUDA_TRY(cudaMemcpyAsync(s->h_pool + (size_t)(r->hbase + r->n_src) * w,
+                                     s->d_pool + (size_t)(r->base + NREG + r->n_src) * w, (size_t)r->n_dst * w * 8,
+                                     cudaMemcpyDeviceToHost, s->alu_stream));
+        CUDA_TRY(cudaEventCreateWithFlags(&r->retired, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventRecord(r->retired, s->alu_stream));
+        s->retiring.push_back(r);
+        progress = true;
     }
     s->active.swap(still);
+    // ready PBS on idle lanes (one many-LUT factor per batch)
+    for (Lane &ln : s->lanes) {
+        if (ln.busy) continue;
+        uint32_t mlk = 0, B = 0;
+        for (Request *r : s->active)
+            for (int i : r->ready)
+                if (r->prog[i].kind == 1 && !mlk) mlk = r->prog[i].mlk;
+        if (!mlk) break;
+        for (Request *r : s->active) {
+            std::vector<int> keep;
+            for (int i : r->ready) {
+                Instr &in = r->prog[i];
+                if (in.kind == 1 && in.mlk == mlk && B < s->max_pbs) {
+                    ln.h_idx[B] = r->base + in.a;
+                    ln.h_idx[s->max_pbs + B] = r->base + in.dst;
+                    ln.h_idx[2 * s->max_pbs + B] = in.gid;
+                    ln.ops.push_back({r, i});
+                    B++;
+                } else {
+                    keep.push_back(i);
+                }
+            }
+            r->ready.swap(keep);
+        }
+        CUDA_TRY(cudaStreamWaitEvent(ln.stream, s->alu_done, 0));
+        CUDA_TRY(cudaMemcpyAsync(ln.d_idx, ln.h_idx, (size_t)s->max_pbs * 3 * 4, cudaMemcpyHostToDevice, ln.stream));
+        CUDA_TRY(launch_keyswitch(s->d_pool, c->d_ksk, nullptr, ln.d_l2n, B, n, c->xpad, ln.stream, ln.d_idx));
+        CUDA_TRY(launch_blind_rotate(c->br, c->nsm, ln.d_l2n, c->d_luts, ln.d_idx + 2 * s->max_pbs, c->nlut,
+                                     c->d_bsk, c->d_tw, s->d_pool, B, n, c->d_err, ln.stream,
+                                     ln.d_idx + s->max_pbs, mlk));
+        CUDA_TRY(cudaEventRecord(ln.done, ln.stream));
+        ln.busy = true;
+        s->launches += 2;
+        s->pbs_done += B;
+        s->rounds++;
+        progress = true;
+    }
+    if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(100));  // GPU busy: do not spin
     if (n_completed) *n_completed = completed;
-    if (n_active) *n_active = (uint32_t)s->active.size();
+    if (n_active) *n_active = (uint32_t)(s->active.size() + s->retiring.size());
     if (n_pending) *n_pending = (uint32_t)s->pending.size();
     return LUTHE_OK;
 }
@@ -456,9 +551,11 @@ extern "C" int luthe_server_fetch(luthe_server *s, uint64_t id, uint64_t *h_dst,
     auto it = s->done.find(id);
     if (it == s->done.end()) return fail(LUTHE_E_STATE, "request %llu is not complete", (unsigned long long)id);
     Request *r = it->second;
-    if (h_dst) memcpy(h_dst, r->h_dst.data(), r->h_dst.size() * 8);
+    const size_t w = s->ctx->p.poly_size + 1;
+    if (h_dst) memcpy(h_dst, s->h_pool + (size_t)(r->hbase + r->n_src) * w, (size_t)r->n_dst * w * 8);
     if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
     if (queue_s) *queue_s = std::chrono::duration<double>(r->t_admit - r->t_submit).count();
+    s->host.release(r->hbase, r->n_src + r->n_dst);
     s->done.erase(it);
     delete r;
     return LUTHE_OK;
@@ -470,7 +567,7 @@ extern "C" int luthe_server_counters(luthe_server *s, uint64_t *rounds, uint64_t
     if (!s) return fail(LUTHE_E_PARAM, "null server");
     if (rounds) *rounds = s->rounds;
     if (pbs) *pbs = s->pbs_done;
-    if (alu) *alu = s->alu_done;
+    if (alu) *alu = s->alu_done_n;
     if (launches) *launches = s->launches;
     return LUTHE_OK;
 }
