@@ -166,7 +166,7 @@ def max_over_ranks(x, dist, device):
     return float(t.item())
 
 
-def serving(L, eng, params, keys, seed, n_req=400, rate=150.0):
+def serving(L, eng, params, keys, seed, n_req=400, rate=300.0):
     """Serving loop under Poisson arrivals of 16-bit radix IOps (50 % ADD with
     carry propagation, 30 % scalar compare, 20 % multiply); every result is
     checked by decryption."""
