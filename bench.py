@@ -383,6 +383,46 @@ def main():
     e2e_verified = bool(np.array_equal(L.decrypt(params, keys["glwe_key"], hout), expect))
     e2e_val = world * B / (max_over_ranks(statistics.mean(e2e_ms), dist, "cuda") * 1e-3)
 
+    # ---- the other configurations: standalone NTT product and key switch
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for r in range(reps):
+            flush.fill_(r)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            fn()
+            a1.record(stream)
+            a1.synchronize()
+            ts.append(a0.elapsed_time(a1))
+        return statistics.median(ts)
+
+    P = 0xFFFFFFFF00000001
+    g = torch.Generator(device="cuda").manual_seed(args.seed)
+    pa = torch.randint(0, 2**62, (4096, 2048), dtype=torch.int64, device="cuda", generator=g)
+    pb = torch.randint(0, 2**62, (4096, 2048), dtype=torch.int64, device="cuda", generator=g)
+    po = torch.empty_like(pa)
+    ntt_ms = timed(lambda: eng.ntt_mul(pa, pb, po, 4096, stream))
+    del pa, pb, po
+    ks_in = torch.randint(-2**62, 2**62, (16384, 2049), dtype=torch.int64, device="cuda", generator=g)
+    ks_o21 = torch.empty((16384, params.lwe_dim + 1), dtype=torch.int32, device="cuda")
+    ks_o2n = torch.empty_like(ks_o21)
+    ks_ms = timed(lambda: eng.keyswitch(ks_in, ks_o21, ks_o2n, 16384, stream))
+    del ks_in, ks_o21, ks_o2n
+    other = {
+        "ntt_product_4096_pairs": {
+            "ms": ntt_ms, "pairs_per_s": 4096 / (ntt_ms * 1e-3),
+            "modmul_per_s": 4096 * 35840 / (ntt_ms * 1e-3),
+            "hbm_gbs_algorithmic": 4096 * 3 * 2048 * 8 / (ntt_ms * 1e-3) / 1e9,
+            "note": "N=2048 pairs, uniform in [0,2^62); 3 transforms + product per pair"},
+        "keyswitch_16384": {
+            "ms": ks_ms, "ciphertexts_per_s": 16384 / (ks_ms * 1e-3),
+            "mac_per_s": 16384 * KS_MAC_PER_BOOTSTRAP / (ks_ms * 1e-3),
+            "imad_frac_of_measured_peak": 16384 * KS_MAC_PER_BOOTSTRAP / (ks_ms * 1e-3) / imad_peak,
+            "note": "16384 BLWEs of dimension 2048 -> n=804, KSK 3x6 mod 2^21"},
+    }
+
     # ---- serving loop (one GPU): Poisson arrivals of radix IOps
     serve = serving(L, eng, params, keys, args.seed + 99) if world == 1 and not args.no_serving else None
 
@@ -427,6 +467,7 @@ def main():
             "clocks": clk,
             "autotune": tune.get("chosen"),
             "serving": serve,
+            "other_configs": other,
         }
         print(json.dumps(line), flush=True)
     eng.close()
