@@ -24,7 +24,8 @@
  *    (the order of the reference's input/output BLWE test vectors).
  *  - KSK:  u32 words mod 2^ks_width, index (x*(k*N) + y)*ks_level + z, x in
  *    [0, n] (the body column last), y the BLWE mask coefficient, z the level
- *    (z = 0 is the least significant digit, weight 2^(ks_base_log*(z+1)))
+ *    (z = 0 is the least significant digit, weight
+ *    2^(ks_width - ks_base_log*(ks_level-z)))
  *    -- the order of the reference's ksk_hwo files with one channel.
  *  - BSK:  standard domain over Z_p, p = 2^64 - 2^32 + 1 (values < p), index
  *    ((i*2 + row)*2 + col)*N + c: GGSW of LWE-key bit i, row = decomposed GLWE

@@ -119,6 +119,31 @@ def default_params(**over):
     return p
 
 
+# The reference's HPU parameter sets (hw/module/param/module/<name>/rtl/
+# param_tfhe_definition_pkg.sv: N, GLWE_K, PBS_L, PBS_B_W, LWE_K, KS_L, KS_B_W,
+# MOD_KSK_W).  All have N = 2048, k = 1, one PBS level, KSK modulus 2^21 and a
+# 2-bit message + 2-bit carry payload.  "default" is the n = 804, KS 3 x 6 set
+# that the gtv model runs by default and the benchmark is quoted on.
+PARAM_SETS = {
+    "default": dict(lwe_dim=804, pbs_base_log=23, ks_base_log=3, ks_level=6),
+    # param_msg2_carry2_pfail64_132b_gaussian_1f72dba/rtl/param_tfhe_definition_pkg.sv:31-53
+    "msg2_carry2_pfail64_132b_gaussian_1f72dba": dict(lwe_dim=804, pbs_base_log=23, ks_base_log=2, ks_level=8),
+    # param_msg2_carry2_pfail64_132b_tuniform_7e47d8c/rtl/param_tfhe_definition_pkg.sv:31-53
+    "msg2_carry2_pfail64_132b_tuniform_7e47d8c": dict(lwe_dim=839, pbs_base_log=23, ks_base_log=2, ks_level=7),
+    # param_msg2_carry2_gaussian/rtl/param_tfhe_definition_pkg.sv:42-64
+    "msg2_carry2_gaussian": dict(lwe_dim=834, pbs_base_log=23, ks_base_log=3, ks_level=5),
+    # param_msg2_carry2_tuniform/rtl/param_tfhe_definition_pkg.sv:38-60
+    "msg2_carry2_tuniform": dict(lwe_dim=887, pbs_base_log=22, ks_base_log=3, ks_level=5),
+}
+
+
+def param_set(name):
+    """Params of one of the reference's named parameter sets (PARAM_SETS)."""
+    if name not in PARAM_SETS:
+        raise KeyError(f"unknown parameter set {name!r}; known: {sorted(PARAM_SETS)}")
+    return default_params(**PARAM_SETS[name])
+
+
 def _ptr(a):
     if a is None:
         return None

@@ -43,10 +43,11 @@ extern "C" void luthe_params_default(luthe_params *p)
 static int check_params(const luthe_params *p)
 {
     if (!p) return fail(LUTHE_E_PARAM, "null params");
-    if (p->glwe_dim != 1 || p->poly_size != (uint32_t)N || p->pbs_base_log != 23 || p->pbs_level != 1 ||
-        p->ks_base_log != (uint32_t)KS_BL || p->ks_level != (uint32_t)KS_L || p->ks_width != (uint32_t)KS_W)
+    if (p->glwe_dim != 1 || p->poly_size != (uint32_t)N || !pbs_supported(p->pbs_base_log) || p->pbs_level != 1 ||
+        !ks_supported(p->ks_base_log, p->ks_level) || p->ks_width != (uint32_t)KS_W)
         return fail(LUTHE_E_PARAM,
-                    "unsupported parameter set (engine is built for k=1 N=2048 PBS 23x1 KS 3x6 mod 2^21)");
+                    "unsupported parameter set (engine is built for k=1 N=2048, PBS 2^23 or 2^22 x 1, "
+                    "KS 3x6, 3x5, 2x8 or 2x7 mod 2^21)");
     if (p->lwe_dim == 0 || p->lwe_dim > 4096) return fail(LUTHE_E_PARAM, "lwe_dim %u out of range", p->lwe_dim);
     if (p->msg_width + p->carry_width + 1 > 32) return fail(LUTHE_E_PARAM, "message width too large");
     return LUTHE_OK;
@@ -118,7 +119,7 @@ extern "C" void luthe_ctx_destroy(luthe_ctx *c)
     dfree(c, c->d_tw, 4096 * 8);
     dfree(c, c->d_err, 4);
     dfree(c, c->d_bsk, n * SLAB_BYTES);
-    dfree(c, c->d_ksk, (size_t)N * KS_L * c->xpad * 4);
+    dfree(c, c->d_ksk, (size_t)N * c->p.ks_level * c->xpad * 4);
     dfree(c, c->d_luts, (size_t)c->nlut * 2 * N * 8);
     dfree(c, c->d_lwe2N, c->cap * (n + 1) * 4);
     dfree(c, c->d_hin, c->hcap * (N + 1) * 8);
@@ -152,7 +153,7 @@ extern "C" int luthe_upload_ksk(luthe_ctx *c, const uint32_t *h)
 {
     if (!c || !h) return fail(LUTHE_E_PARAM, "null argument");
     CUDA_TRY(cudaSetDevice(c->device));
-    const size_t n = c->p.lwe_dim, K = (size_t)N * KS_L;
+    const size_t n = c->p.lwe_dim, K = (size_t)N * c->p.ks_level;
     const uint32_t xpad = (uint32_t)(((n + 1) + KS_BN - 1) / KS_BN * KS_BN);
     std::vector<uint32_t> t((size_t)K * xpad, 0);
     const uint32_t M = (1u << KS_W) - 1;
@@ -215,9 +216,9 @@ static int enqueue_ks_pbs(luthe_ctx *c, const uint64_t *d_in, const uint32_t *d_
                           cudaStream_t s)
 {
     const uint32_t n = c->p.lwe_dim;
-    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s));
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level));
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out,
-                                 count, n, c->d_err, s));
+                                 count, n, c->d_err, s, nullptr, 1, c->p.pbs_base_log));
     return LUTHE_OK;
 }
 
@@ -245,9 +246,9 @@ extern "C" int luthe_ks_pbs_ml(luthe_ctx *c, const uint64_t *d_in, const uint32_
     if ((r = ensure_scratch(c, count))) return r;
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t n = c->p.lwe_dim;
-    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s));
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level));
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out, count,
-                                 n, c->d_err, s, nullptr, mlk));
+                                 n, c->d_err, s, nullptr, mlk, c->p.pbs_base_log));
     return LUTHE_OK;
 }
 
@@ -329,7 +330,7 @@ extern "C" int luthe_keyswitch(luthe_ctx *c, const uint64_t *d_in, uint32_t *d_o
     if (!d_in || !d_out2N) return fail(LUTHE_E_PARAM, "null buffer");
     CUDA_TRY(cudaSetDevice(c->device));
     CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, d_out21, d_out2N, count, c->p.lwe_dim, c->xpad,
-                              (cudaStream_t)stream));
+                              (cudaStream_t)stream, nullptr, c->p.ks_base_log, c->p.ks_level));
     return LUTHE_OK;
 }
 
@@ -342,7 +343,7 @@ extern "C" int luthe_blind_rotate(luthe_ctx *c, const uint32_t *d_lwe2N, const u
     if (!d_lwe2N || !d_ids || !d_out) return fail(LUTHE_E_PARAM, "null buffer");
     CUDA_TRY(cudaSetDevice(c->device));
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out, count,
-                                 c->p.lwe_dim, c->d_err, (cudaStream_t)stream));
+                                 c->p.lwe_dim, c->d_err, (cudaStream_t)stream, nullptr, 1, c->p.pbs_base_log));
     return LUTHE_OK;
 }
 
@@ -451,11 +452,11 @@ extern "C" int luthe_autotune(luthe_ctx *c, size_t sample, char *json, size_t ca
         cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
         if ((size_t)max_smem < cfg.ctas_per_sm * (smem + 1024)) continue;
         cudaError_t e = launch_blind_rotate(cfg, c->nsm, d_l, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_o,
-                                            sample, n, c->d_err, 0);
+                                            sample, n, c->d_err, 0, nullptr, 1, c->p.pbs_base_log);
         cudaEventRecord(e0, 0);
         for (int rep = 0; rep < 2 && e == cudaSuccess; rep++)
             e = launch_blind_rotate(cfg, c->nsm, d_l, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_o, sample, n,
-                                    c->d_err, 0);
+                                    c->d_err, 0, nullptr, 1, c->p.pbs_base_log);
         cudaEventRecord(e1, 0);
         if (e == cudaSuccess) e = cudaEventSynchronize(e1);
         if (e != cudaSuccess) {
@@ -543,8 +544,8 @@ extern "C" int luthe_ks_pbs_noalloc(luthe_ctx *c, const uint64_t *d_in, const ui
     uint32_t *scratch = g_noalloc_addr[c->device];
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t n = c->p.lwe_dim;
-    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, scratch, count, n, c->xpad, s));
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, scratch, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level));
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, scratch, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out, count, n,
-                                 c->d_err, s));
+                                 c->d_err, s, nullptr, 1, c->p.pbs_base_log));
     return LUTHE_OK;
 }

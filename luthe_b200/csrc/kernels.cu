@@ -233,32 +233,37 @@ cudaError_t launch_ntt_mul(const uint64_t *d_a, const uint64_t *d_b, uint64_t *d
 //  pep_ks_out_process.sv:276-280,336-341).  A SIMT integer GEMM: M = ciphertexts,
 // N = output coefficients, K = (y, z) pairs.  The digits (in [-4, 4]) are made
 // on the fly from the 64-bit mask coefficients; 32-bit wrap-around keeps the
-// low 21 bits exact.  KSK is transposed to [y*L+z][x] on upload.
+// low 21 bits exact.  KSK is transposed to [y*L+z][x] on upload.  Templated
+// on the decomposition (base 2^BL, L levels) of the reference's parameter sets.
+template <int BL, int L>
 __device__ __forceinline__ void ks_decomp(u64 v, int *d)
 {
-    // base 2^3, 6 levels: closest_rep = top 18 bits + round bit; tie rule of
+    // closest_rep = top BL*L bits + round bit; tie rule of
     // balanced_decomp_unfix_sign_round_bit.py:42-101 / decomp_parallel.sv:73-75,142-150
-    u32 rb = (u32)(v >> 45) & 1u;
-    u32 c = (u32)(v >> 46) + rb;  // 0 .. 2^18
-    u32 last_sign = ((c >> 17) & 1u) && ((c & 0x1FFFFu) || rb);
+    constexpr int TOT = BL * L;
+    constexpr u32 MASK = (1u << BL) - 1, HALF = 1u << (BL - 1);
+    u32 rb = (u32)(v >> (63 - TOT)) & 1u;
+    u32 c = (u32)(v >> (64 - TOT)) + rb;  // 0 .. 2^TOT
+    u32 last_sign = ((c >> (TOT - 1)) & 1u) && ((c & ((1u << (TOT - 1)) - 1)) || rb);
     u32 carry = 0;
 #pragma unroll
-    for (int i = 0; i < KS_L; i++) {
-        u32 raw = (c >> (3 * i)) & 7u;
-        u32 nxt = (i + 1 < KS_L) ? ((c >> (3 * (i + 1))) & 7u) : (last_sign ? 7u : 0u);
+    for (int i = 0; i < L; i++) {
+        u32 raw = (c >> (BL * i)) & MASK;
+        u32 nxt = (i + 1 < L) ? ((c >> (BL * (i + 1))) & MASK) : (last_sign ? MASK : 0u);
         u32 tv = raw + carry;
-        bool negd = (tv >> 3) || ((tv & 4u) && ((tv & 3u) || (nxt & 4u)));
-        d[i] = negd ? (int)tv - 8 : (int)tv;
+        bool negd = (tv >> BL) || ((tv & HALF) && ((tv & (HALF - 1)) || (nxt & HALF)));
+        d[i] = negd ? (int)tv - (1 << BL) : (int)tv;
         carry = negd ? 1u : 0u;
     }
 }
 
+template <int BL, int L>
 __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, const u32 *__restrict__ src_idx,
                                                   const u32 *__restrict__ ksk_t, u32 *__restrict__ out21,
                                                   u32 *__restrict__ out2N, u32 B, u32 n, u32 xpad)
 {
-    __shared__ __align__(16) int dsm[KS_KC * KS_L][KS_BM];  // digits [k][ct]
-    __shared__ __align__(16) u32 ksm[KS_KC * KS_L][KS_BN];  // KSK tile [k][x]
+    __shared__ __align__(16) int dsm[KS_KC * L][KS_BM];  // digits [k][ct]
+    __shared__ __align__(16) u32 ksm[KS_KC * L][KS_BN];  // KSK tile [k][x]
     const int tid = threadIdx.x;
     const int ty = tid >> 5, tx = tid & 31;  // 8 x 4 cts, 32 x 4 outputs
     const u32 c0 = blockIdx.y * KS_BM, x0 = blockIdx.x * KS_BN;
@@ -273,21 +278,21 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
     const size_t dct_g = src_idx ? src_idx[dct_c] : dct_c;  // row of the input array
     for (u32 y0 = 0; y0 < (u32)N; y0 += KS_KC) {
         {
-            int d[KS_L];
-            ks_decomp(in[(size_t)dct_g * (N + 1) + y0 + dy], d);
+            int d[L];
+            ks_decomp<BL, L>(in[(size_t)dct_g * (N + 1) + y0 + dy], d);
 #pragma unroll
-            for (int z = 0; z < KS_L; z++) dsm[dy * KS_L + z][dct] = d[z];
+            for (int z = 0; z < L; z++) dsm[dy * L + z][dct] = d[z];
         }
-        const uint4 *src = reinterpret_cast<const uint4 *>(ksk_t + (size_t)y0 * KS_L * xpad + x0);
+        const uint4 *src = reinterpret_cast<const uint4 *>(ksk_t + (size_t)y0 * L * xpad + x0);
 #pragma unroll
-        for (int r = 0; r < (KS_KC * KS_L * KS_BN / 4) / 256; r++) {
+        for (int r = 0; r < (KS_KC * L * KS_BN / 4) / 256; r++) {
             int idx = tid + r * 256;
             int k = idx / (KS_BN / 4), xv = idx % (KS_BN / 4);
             reinterpret_cast<uint4 *>(&ksm[k][0])[xv] = src[(size_t)k * (xpad / 4) + xv];
         }
         __syncthreads();
 #pragma unroll 8
-        for (int k = 0; k < KS_KC * KS_L; k++) {
+        for (int k = 0; k < KS_KC * L; k++) {
             int4 dv = reinterpret_cast<const int4 *>(&dsm[k][0])[ty];
             uint4 kv = reinterpret_cast<const uint4 *>(&ksm[k][0])[tx];
             int dd[4] = {dv.x, dv.y, dv.z, dv.w};
@@ -317,12 +322,23 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
     }
 }
 
+bool ks_supported(uint32_t bl, uint32_t L)
+{
+    return (bl == 3 && (L == 6 || L == 5)) || (bl == 2 && (L == 8 || L == 7));
+}
+
 cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21, uint32_t *d_out2N,
-                             size_t B, uint32_t n, uint32_t xpad, cudaStream_t s, const uint32_t *d_src_idx)
+                             size_t B, uint32_t n, uint32_t xpad, cudaStream_t s, const uint32_t *d_src_idx,
+                             uint32_t bl, uint32_t L)
 {
     if (B == 0) return cudaSuccess;
     dim3 grid(xpad / KS_BN, (unsigned)((B + KS_BM - 1) / KS_BM));
-    ks_kernel<<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, (u32)B, n, xpad);
+    const u32 Bu = (u32)B;
+    if (bl == 3 && L == 6) ks_kernel<3, 6><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, Bu, n, xpad);
+    else if (bl == 3 && L == 5) ks_kernel<3, 5><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, Bu, n, xpad);
+    else if (bl == 2 && L == 8) ks_kernel<2, 8><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, Bu, n, xpad);
+    else if (bl == 2 && L == 7) ks_kernel<2, 7><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, Bu, n, xpad);
+    else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 
@@ -388,7 +404,7 @@ __device__ __forceinline__ void issue_slab(u64 *slab, const u64 *src, u64 *mbar)
     for (int c = 0; c < 4; c++) bulk_g2s(slab + c * (SLAB_WORDS / 4), src + c * (SLAB_WORDS / 4), SLAB_BYTES / 4, mbar);
 }
 
-template <int G>
+template <int G, int BW>
 __global__ void __launch_bounds__(G * 256, 1)
     br_kernel(const u32 *__restrict__ lwe2N, const u64 *__restrict__ luts, const u32 *__restrict__ lut_id, u32 nlut,
               const u64 *__restrict__ bsk, const u64 *__restrict__ tw, u64 *__restrict__ out, u32 B, u32 n,
@@ -446,7 +462,7 @@ __global__ void __launch_bounds__(G * 256, 1)
                     const u32 src = (j + TWO_N - a) & (TWO_N - 1);
                     u64 v = buf[q * POLY_WORDS + (src & (N - 1))];
                     if (src >= (u32)N) v = 0ull - v;
-                    x[q][e] = gl::decomp23_to_p(v - acc[q][e]);
+                    x[q][e] = gl::decomp_to_p<BW>(v - acc[q][e]);
                 }
             ntt::group_sync(bar);
             ntt::forward<2>(x, buf, tws, t, bar);
@@ -513,18 +529,21 @@ size_t br_smem_bytes(const BrConfig &cfg, uint32_t n)
     return (size_t)(SLAB_WORDS + 4096 + G * 2 * POLY_WORDS + 2) * 8 + (size_t)G * (n + 1) * 4;
 }
 
-template <int G>
+template <int G, int BW>
 static cudaError_t br_attr(size_t smem)
 {
-    return cudaFuncSetAttribute(br_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return cudaFuncSetAttribute(br_kernel<G, BW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
+
+bool pbs_supported(uint32_t bw) { return bw == 23 || bw == 22; }
 
 cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n)
 {
     size_t smem = br_smem_bytes(cfg, n);
+    cudaError_t e;
     switch (cfg.cts_per_cta) {
-    case 1: return br_attr<1>(smem);
-    case 2: return br_attr<2>(smem);
+    case 1: e = br_attr<1, 23>(smem); return e != cudaSuccess ? e : br_attr<1, 22>(smem);
+    case 2: e = br_attr<2, 23>(smem); return e != cudaSuccess ? e : br_attr<2, 22>(smem);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -532,7 +551,7 @@ cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n)
 cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_lwe2N, const uint64_t *d_luts,
                                 const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
                                 uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s,
-                                const uint32_t *d_dst_idx, uint32_t mlk)
+                                const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw)
 {
     if (B == 0) return cudaSuccess;
     if (mlk != 1 && mlk != 2 && mlk != 4 && mlk != 8) return cudaErrorInvalidValue;
@@ -545,11 +564,12 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
     void *args[] = {(void *)&d_lwe2N, (void *)&d_luts, (void *)&d_lut_id, (void *)&nlut, (void *)&d_bsk,
                     (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err,
                     (void *)&d_dst_idx, (void *)&mlk};
-    switch (G) {
-    case 1: return cudaLaunchKernel((const void *)br_kernel<1>, dim3((unsigned)grid), dim3(256), args, smem, s);
-    case 2: return cudaLaunchKernel((const void *)br_kernel<2>, dim3((unsigned)grid), dim3(512), args, smem, s);
-    default: return cudaErrorInvalidValue;
-    }
+    const void *k;
+    if (G == 1) k = pbs_bw == 22 ? (const void *)br_kernel<1, 22> : (const void *)br_kernel<1, 23>;
+    else if (G == 2) k = pbs_bw == 22 ? (const void *)br_kernel<2, 22> : (const void *)br_kernel<2, 23>;
+    else return cudaErrorInvalidValue;
+    if (!pbs_supported(pbs_bw)) return cudaErrorInvalidValue;
+    return cudaLaunchKernel(k, dim3((unsigned)grid), dim3(256 * G), args, smem, s);
 }
 
 // ---------------------------------------------------------- linear DOps

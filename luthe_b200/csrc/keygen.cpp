@@ -67,7 +67,8 @@ extern "C" int luthe_keygen(const luthe_params *p, uint64_t seed, uint32_t *lwe_
     for (uint32_t i = 0; i < n; i++) lwe_key[i] = rnd(seed, S_LWE_KEY, i) & 1;
     for (uint32_t j = 0; j < N; j++) glwe_key[j] = rnd(seed, S_GLWE_KEY, j) & 1;
 
-    // KSK[x][y][z]: LWE_s( S_y * 2^(bl*(z+1)) ) mod 2^W  (pep_ks_mult_node.sv operands)
+    // KSK[x][y][z]: LWE_s( S_y * 2^(W - bl*(L-z)) ) mod 2^W: level z = L-1 is the
+    // most significant digit, weight 2^(W-bl) (pep_ks_mult_node.sv operands)
     const uint32_t M = W == 32 ? 0xFFFFFFFFu : ((1u << W) - 1);
     const double ks_sigma = LWE_SIGMA_REL * ldexp(1.0, (int)W);
 #pragma omp parallel for schedule(static)
@@ -80,7 +81,7 @@ extern "C" int luthe_keygen(const luthe_params *p, uint64_t seed, uint32_t *lwe_
             body += a * lwe_key[x];
         }
         body += (uint32_t)gauss(seed, S_KSK_NOISE, yz, ks_sigma);
-        body += glwe_key[y] << (bl * (z + 1));
+        body += glwe_key[y] << (W - bl * (L - z));
         ksk[((size_t)n * N + y) * L + z] = body & M;
     }
 

@@ -56,15 +56,15 @@ def bitrev(x, bits):
     return int(format(x, "0%db" % bits)[::-1], 2)
 
 
-def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120):
+def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120, ks_bl=3, ks_lc=6, pbs_bl=23):
     gtv = os.path.join(ref, "sw/bin/gtv/v1.4.1/gtv")
     out = tempfile.mkdtemp(prefix="gtv_")
     lwe_sd, glwe_sd = noise
     # gtv searches for NTT roots unless given; pass the ones the reference's
     # simulation flow uses (run.sh:429-458): phi = psi^(2048/N), omega = phi^2
     phi = pow(0x984ec5194d005735, 2048 // N, P)
-    cmd = [gtv, "--omega-ru-n", str(phi * phi % P), "--phi-ru-2n", str(phi), "--lwe-dim", str(n), "--glwe-dim", "1", "--poly-size", str(N), "--pbs-bl", "23", "--pbs-lc", "1",
-           "--ks-bl", "3", "--ks-lc", "6", "--ct-w", "64", "--ks-w", "21", "--msg-w", "2", "--carry-w", "2",
+    cmd = [gtv, "--omega-ru-n", str(phi * phi % P), "--phi-ru-2n", str(phi), "--lwe-dim", str(n), "--glwe-dim", "1", "--poly-size", str(N), "--pbs-bl", str(pbs_bl), "--pbs-lc", "1",
+           "--ks-bl", str(ks_bl), "--ks-lc", str(ks_lc), "--ct-w", "64", "--ks-w", "21", "--msg-w", "2", "--carry-w", "2",
            "--pbs-batch", "1", "--pbs-per-batch", str(per_batch), "--seed", str(seed), "--ntt-radix", "2",
            "--psi", "4", "--ntt-delta", "3", "--lwe-std-dev", repr(lwe_sd), "--glwe-std-dev", repr(glwe_sd),
            "--ksk-pc", "1", "--bsk-pc", "1", "--ks-lbx", "1", "--ks-lby", "1", "--ks-lbz", "1",
@@ -89,6 +89,7 @@ def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120):
     names = sorted(ins, key=lambda s: int(s[4:]))
     fx = {
         "n": n, "N": N, "seed": seed, "lwe_std_dev": lwe_sd, "glwe_std_dev": glwe_sd,
+        "ks_bl": ks_bl, "ks_lc": ks_lc, "pbs_bl": pbs_bl,
         "lwe_key": np.array(key, np.uint32),
         "msgs": np.array(msgs, np.uint32),
         "ksk": np.array(ksk, np.uint32),
@@ -191,6 +192,11 @@ if __name__ == "__main__":
         run_gtv(ref, "n8_N64_noiseless", 8, 64, 4, 7, (0.0, 0.0))
         run_gtv(ref, "n32_N256", 32, 256, 6, 11, (5.3943e-6, 4.4409e-16))
         run_gtv(ref, "n32_N2048", 32, 2048, 3, 13, (5.3943e-6, 4.4409e-16))
+        # decompositions of the reference's other parameter sets
+        run_gtv(ref, "n32_N256_ks2x8", 32, 256, 6, 17, (5.3943e-6, 4.4409e-16), ks_bl=2, ks_lc=8)
+        run_gtv(ref, "n32_N256_ks2x7", 32, 256, 6, 19, (5.3943e-6, 4.4409e-16), ks_bl=2, ks_lc=7)
+        run_gtv(ref, "n32_N256_ks3x5", 32, 256, 6, 23, (5.3943e-6, 4.4409e-16), ks_bl=3, ks_lc=5)
+        run_gtv(ref, "n32_N256_ks3x5_pbs22", 32, 256, 6, 29, (5.3943e-6, 4.4409e-16), ks_bl=3, ks_lc=5, pbs_bl=22)
     decomposer_vectors(ref)
     monomial_vectors(ref)
     solinas_vectors(ref)

@@ -73,13 +73,17 @@ def test_keygen_is_deterministic(params):
     assert np.all(a["bsk"] < np.uint64(0xFFFFFFFF00000001))
 
 
-def test_ksk_encrypts_key_digits(params, keys):
-    # KSK[x][y][z] is an LWE encryption of S_y 2^(3(z+1)) mod 2^21 under the small key
-    n, N = params.lwe_dim, params.poly_size
-    K = keys["ksk"].reshape(n + 1, N, 6).astype(np.int64)
+@pytest.mark.parametrize("name", ["default", "msg2_carry2_pfail64_132b_gaussian_1f72dba"])
+def test_ksk_encrypts_key_digits(name):
+    # KSK[x][y][z] is an LWE encryption of S_y 2^(21 - bl(L-z)) mod 2^21 under
+    # the small key: level L-1 carries the most significant digit
+    p = L.param_set(name)
+    keys = L.keygen(p, 20261203)
+    n, N, bl, lc = p.lwe_dim, p.poly_size, p.ks_base_log, p.ks_level
+    K = keys["ksk"].reshape(n + 1, N, lc).astype(np.int64)
     s = keys["lwe_key"].astype(np.int64)
     for y in (0, 1, 1000):
-        for z in range(6):
+        for z in range(lc):
             ph = (K[n, y, z] - int((K[:n, y, z] * s).sum())) % (1 << 21)
-            err = (ph - int(keys["glwe_key"][y]) * (1 << (3 * (z + 1))) + (1 << 20)) % (1 << 21) - (1 << 20)
+            err = (ph - int(keys["glwe_key"][y]) * (1 << (21 - bl * (lc - z))) + (1 << 20)) % (1 << 21) - (1 << 20)
             assert abs(err) < 100

@@ -11,7 +11,14 @@ import luthe_b200 as L
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 P = oracle.P
-GTV_CASES = ["n8_N64_noiseless", "n32_N256", "n32_N2048"]
+GTV_CASES = ["n8_N64_noiseless", "n32_N256", "n32_N2048",
+             # the decompositions of the reference's other parameter sets
+             "n32_N256_ks2x8", "n32_N256_ks2x7", "n32_N256_ks3x5", "n32_N256_ks3x5_pbs22"]
+
+
+def ks_of(g):
+    """(base log, levels) of a fixture's key switch (3 x 6 where not recorded)."""
+    return (int(g["ks_bl"]), int(g["ks_lc"])) if "ks_bl" in g else (3, 6)
 
 
 def gold(name):
@@ -81,21 +88,25 @@ def test_ntt_eval_definition():
 
 
 def _glwe_key_from_ksk(g):
-    """Recover the big key S from the KSK's top level (weight 2^18): with the
-    reference's printed small key, body - <mask, s> = S_y 2^18 + small noise."""
+    """Recover the big key S from the KSK's top level (weight 2^(21-bl)): with the
+    reference's printed small key, body - <mask, s> = S_y 2^(21-bl) + small noise."""
     n, N = int(g["n"]), int(g["N"])
+    bl, lc = ks_of(g)
     ksk, s = g["ksk"].astype(np.int64), g["lwe_key"].astype(np.int64)
-    K = ksk.reshape(n + 1, N, 6)[:, :, 5]
+    K = ksk.reshape(n + 1, N, lc)[:, :, lc - 1]
     ph = (K[n] - (K[:n] * s[:, None]).sum(0)) % (1 << 21)
-    return (np.round(ph / 2**18).astype(np.int64) % 8).astype(np.uint32)
+    S = (np.round(ph / 2**(21 - bl)).astype(np.int64) % (1 << bl)).astype(np.uint32)
+    assert set(np.unique(S)) <= {0, 1}
+    return S
 
 
 @pytest.mark.parametrize("case", GTV_CASES)
 def test_keyswitch_bit_exact_vs_reference_vectors(case):
     g = gold(f"gtv_{case}.npz")
     n, N = int(g["n"]), int(g["N"])
+    bl, lc = ks_of(g)
     for ci, s21, s2n in zip(g["blwe_in"], g["inner_slwe"], g["inner_slwe_2N"]):
-        o21, o2n = oracle.keyswitch(ci, g["ksk"], n, N, gtv_top_tie=True)
+        o21, o2n = oracle.keyswitch(ci, g["ksk"], n, N, ks_bl=bl, ks_lc=lc, gtv_top_tie=True)
         assert np.array_equal(o21, s21)
         # the RTL's 2N switch is LWE_COEF_W bits wide (pep_ks_out_process.sv:340-341)
         # and wraps a rounded-up 2N to 0; the generator prints it unreduced
@@ -104,22 +115,24 @@ def test_keyswitch_bit_exact_vs_reference_vectors(case):
 
 @pytest.mark.parametrize("case", GTV_CASES)
 def test_rtl_keyswitch_same_phase_as_reference_vectors(case):
-    # RTL tie rule (the engine's): the two differ by 8 in the top digit at a
-    # tie, i.e. by 8 * KSK[.][y][5]; the phase moves by 8 * (S_y 2^18 + e) = 8e
-    # mod 2^21 (zero for the noiseless vectors), the masks differ
+    # RTL tie rule (the engine's): the two differ by 2^bl in the top digit at a
+    # tie, i.e. by 2^bl * KSK[.][y][L-1]; the phase moves by
+    # 2^bl * (S_y 2^(21-bl) + e) = 2^bl e mod 2^21 (zero for the noiseless
+    # vectors), the masks differ
     g = gold(f"gtv_{case}.npz")
     n, N = int(g["n"]), int(g["N"])
+    bl, lc = ks_of(g)
     s = g["lwe_key"].astype(np.int64)
     noiseless = float(g["lwe_std_dev"]) == 0.0
     for ci, s21 in zip(g["blwe_in"], g["inner_slwe"]):
-        o21, _ = oracle.keyswitch(ci, g["ksk"], n, N)
+        o21, _ = oracle.keyswitch(ci, g["ksk"], n, N, ks_bl=bl, ks_lc=lc)
         ph_ref = (int(s21[n]) - int((s21[:n].astype(np.int64) * s).sum())) % (1 << 21)
         ph_rtl = (int(o21[n]) - int((o21[:n].astype(np.int64) * s).sum())) % (1 << 21)
-        ties = sum(oracle.decompose(int(v), 3, 6) != oracle.decompose(int(v), 3, 6, True) for v in ci[:N])
+        ties = sum(oracle.decompose(int(v), bl, lc) != oracle.decompose(int(v), bl, lc, True) for v in ci[:N])
         diff = (ph_rtl - ph_ref + (1 << 20)) % (1 << 21) - (1 << 20)
         if noiseless:
             assert diff == 0
-        assert abs(diff) <= 8 * 64 * max(ties, 1)
+        assert abs(diff) <= (1 << bl) * 64 * max(ties, 1)
         assert (ties == 0) == np.array_equal(o21, s21)
 
 
@@ -156,3 +169,17 @@ def test_oracle_blind_rotate_identity_rotation(params, keys, oracle_bsk):
     out = oracle_bsk.blind_rotate(np.zeros((1, n + 1), np.uint32), lut, np.zeros(1, np.uint32))[0]
     assert out[0] == lut[0] and out[N] == lut[N]
     assert np.array_equal(out[1:N], (np.uint64(0) - lut[1:N][::-1]))
+
+
+@pytest.mark.parametrize("name", [s for s in L.PARAM_SETS if s != "default"])
+def test_oracle_pbs_decrypts_for_each_parameter_set(name):
+    # keys, oracle KS (the set's base/levels) and PBS (its base) agree end to end
+    p = L.param_set(name)
+    keys = L.keygen(p, 77 + p.lwe_dim)
+    ob = oracle.OracleBsk(keys["bsk"], p.lwe_dim, p.poly_size)
+    table = np.array([(3 * m + 1) % 16 for m in range(16)], np.uint32)
+    msgs = np.array([0, 7, 15], np.uint32)
+    ct = L.encrypt(p, keys["glwe_key"], msgs, 3)
+    out = ob.ks_pbs(keys["ksk"], ct, L.lut_build(p, table), np.zeros(3, np.uint32), ks_bl=p.ks_base_log,
+                    ks_lc=p.ks_level, pbs_bl=p.pbs_base_log)
+    assert [int(x) for x in L.decrypt(p, keys["glwe_key"], out)] == [int(table[m]) for m in msgs]
