@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=48, help="ciphertexts in the CPU-baseline sample")
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop measurement")
+    ap.add_argument("--no-param-sets", action="store_true",
+                    help="skip the KS+PBS measurement of the reference's other parameter sets")
     ap.add_argument("--ncu-case", action="store_true",
                     help="small profiling case: KS+PBS of 296 BLWEs (one persistent wave), twice, then exit")
     return ap.parse_args()
@@ -228,6 +230,46 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0):
             "latency_ms_p50": float(np.percentile(ls, 50)), "latency_ms_p99": float(np.percentile(ls, 99)),
             "rounds": cnt["rounds"], "pbs": cnt["pbs"], "alu_dops": cnt["alu"], "launches": cnt["launches"],
             "results_decrypt_correct": f"{ok}/{n_req}"}
+
+
+def param_set_runs(L, seed, steps, flush, stream):
+    """KS+PBS throughput of each of the reference's other parameter sets on the
+    same 5370-BLWE workload (fresh keys per set), decryption checked."""
+    import torch
+    res = {}
+    for name in L.PARAM_SETS:
+        if name == "default":
+            continue
+        p = L.param_set(name)
+        keys = L.keygen(p, seed)
+        ct, ids, luts, expect = workload(L, p, keys, seed + 1)
+        B = len(ct)
+        eng = L.Engine(p)
+        eng.upload_keys(keys)
+        eng.upload_luts(luts)
+        eng.reserve(B)
+        d_in = torch.from_numpy(ct.view(np.int64)).cuda()
+        d_ids = torch.from_numpy(ids.view(np.int32)).cuda()
+        d_out = torch.empty_like(d_in)
+        eng.ks_pbs(d_in, d_ids, d_out, B, stream)
+        torch.cuda.synchronize()
+        ms = []
+        for k in range(steps):
+            flush.fill_(k)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.ks_pbs(d_in, d_ids, d_out, B, stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        eng.check_device_error()
+        ok = bool(np.array_equal(L.decrypt(p, keys["glwe_key"], d_out.cpu().numpy().view(np.uint64)), expect))
+        res[name] = {"lwe_dim": p.lwe_dim, "ks": f"{p.ks_base_log}x{p.ks_level}", "pbs_base_log": p.pbs_base_log,
+                     "bootstraps_per_s": B * len(ms) / (sum(ms) * 1e-3), "ms_per_step": statistics.mean(ms),
+                     "verified_decrypt": ok}
+        eng.close()
+        del d_in, d_ids, d_out
+    return res
 
 
 def config_dict():
@@ -423,6 +465,11 @@ def main():
             "note": "16384 BLWEs of dimension 2048 -> n=804, KSK 3x6 mod 2^21"},
     }
 
+    # ---- the reference's other parameter sets (one GPU)
+    psets = None
+    if world == 1 and not args.no_param_sets:
+        psets = param_set_runs(L, args.seed + 7, 3, flush, stream)
+
     # ---- serving loop (one GPU): Poisson arrivals of radix IOps
     serve = serving(L, eng, params, keys, args.seed + 99) if world == 1 and not args.no_serving else None
 
@@ -468,6 +515,7 @@ def main():
             "autotune": tune.get("chosen"),
             "serving": serve,
             "other_configs": other,
+            "param_sets": psets,
         }
         print(json.dumps(line), flush=True)
     eng.close()

@@ -164,8 +164,10 @@ int luthe_lwe_op(luthe_ctx *ctx, int op, const uint64_t *d_a, const uint64_t *d_
  * PBS_ML2/4/8 0x31-0x33 (| 0x08: flush variant).  Each luthe_server_step
  * admits pending requests while the slot pool (carved from the context's HBM
  * budget) has room, issues every ready linear DOp of every request in one
- * launch and every ready PBS of every request in one KS+PBS launch, and
- * retires finished requests.  Latency is measured from submit to retire. */
+ * launch, gathers the ready PBS DOps of every request (one many-LUT factor per
+ * launch) into a KS+PBS launch on each idle PBS lane (own stream and
+ * scratch, so batches overlap on the GPU), and retires finished requests.
+ * Latency is measured from submit to retire. */
 typedef struct luthe_server luthe_server;
 int luthe_server_create(luthe_ctx *ctx, uint64_t pool_bytes, uint32_t max_pbs, luthe_server **out);
 void luthe_server_destroy(luthe_server *srv);
