@@ -272,6 +272,41 @@ def param_set_runs(L, seed, steps, flush, stream):
     return res
 
 
+def cpu_ntt_product(a, b, gpu_out):
+    """Config 1 on the host: the oracle's radix-2 NTT product (C) of the first
+    64 pairs, 1 thread and all threads; bit-checked against the GPU rows."""
+    import oracle
+    res = {"kind": "port", "sample": f"first {len(a)} pairs of the 4096"}
+    for label, th in (("1_thread", 1), ("all_threads", os.cpu_count() or 1)):
+        oracle.set_threads(th)
+        t0 = time.perf_counter()
+        out = oracle.negacyclic_mul(a, b)
+        dt = time.perf_counter() - t0
+        res[label] = {"pairs_per_s": len(a) / dt, "threads": th}
+    res["bit_exact_vs_gpu"] = bool(np.array_equal(out, gpu_out))
+    return res
+
+
+def cpu_keyswitch(blwe, gpu_out21, ksk, params):
+    """Config 3 on the host: the oracle's key switch (C) of the first 64
+    ciphertexts, 1 thread and all threads (one ciphertext per thread)."""
+    import concurrent.futures as cf
+    import oracle
+    n, N = params.lwe_dim, params.poly_size
+    one = lambda c: oracle.keyswitch(blwe[c], ksk, n, N)[0]
+    res = {"kind": "port", "sample": f"first {len(blwe)} ciphertexts of the 16384"}
+    t0 = time.perf_counter()
+    outs = [one(c) for c in range(len(blwe))]
+    res["1_thread"] = {"ciphertexts_per_s": len(blwe) / (time.perf_counter() - t0), "threads": 1}
+    th = os.cpu_count() or 1
+    with cf.ThreadPoolExecutor(th) as ex:                 # the C call releases the GIL
+        t0 = time.perf_counter()
+        list(ex.map(one, range(len(blwe))))
+        res["all_threads"] = {"ciphertexts_per_s": len(blwe) / (time.perf_counter() - t0), "threads": th}
+    res["bit_exact_vs_gpu"] = bool(np.array_equal(np.stack(outs), gpu_out21))
+    return res
+
+
 def config_dict():
     return {
         "workload": "batched KS+PBS of uneven batches 1+17+256+1000+4096 = 5370 BLWEs in one launch, "
@@ -446,11 +481,14 @@ def main():
     pb = torch.randint(0, 2**62, (4096, 2048), dtype=torch.int64, device="cuda", generator=g)
     po = torch.empty_like(pa)
     ntt_ms = timed(lambda: eng.ntt_mul(pa, pb, po, 4096, stream))
+    ntt_sample = (pa[:64].cpu().numpy().view(np.uint64), pb[:64].cpu().numpy().view(np.uint64),
+                  po[:64].cpu().numpy().view(np.uint64))
     del pa, pb, po
     ks_in = torch.randint(-2**62, 2**62, (16384, 2049), dtype=torch.int64, device="cuda", generator=g)
     ks_o21 = torch.empty((16384, params.lwe_dim + 1), dtype=torch.int32, device="cuda")
     ks_o2n = torch.empty_like(ks_o21)
     ks_ms = timed(lambda: eng.keyswitch(ks_in, ks_o21, ks_o2n, 16384, stream))
+    ks_sample = (ks_in[:64].cpu().numpy().view(np.uint64), ks_o21[:64].cpu().numpy().view(np.uint32))
     del ks_in, ks_o21, ks_o2n
     other = {
         "ntt_product_4096_pairs": {
@@ -469,6 +507,12 @@ def main():
     psets = None
     if world == 1 and not args.no_param_sets:
         psets = param_set_runs(L, args.seed + 7, 3, flush, stream)
+
+    # CPU restatements of configs 1 and 3 (the oracle, C; 1 thread and all
+    # host threads) on bounded samples, checked against the GPU rows
+    if rank == 0 and world == 1 and args.cpu_sample > 0:
+        other["ntt_product_4096_pairs"]["cpu"] = cpu_ntt_product(*ntt_sample)
+        other["keyswitch_16384"]["cpu"] = cpu_keyswitch(*ks_sample, keys["ksk"], params)
 
     # ---- serving loop (one GPU): Poisson arrivals of radix IOps
     serve = serving(L, eng, params, keys, args.seed + 99) if world == 1 and not args.no_serving else None

@@ -397,6 +397,20 @@ __device__ __forceinline__ bool mbar_wait(u64 *mbar, u32 parity)
     return false;
 }
 
+// named-barrier OR-reduction over one 256-thread ciphertext group
+__device__ __forceinline__ bool group_sync_or(int bar_id, bool pred)
+{
+    u32 r;
+    asm volatile("{\n\t.reg .pred p, q;\n\t"
+                 "setp.ne.u32 p, %1, 0;\n\t"
+                 "barrier.cta.red.or.pred q, %2, %3, p;\n\t"
+                 "selp.u32 %0, 1, 0, q;\n\t}"
+                 : "=r"(r)
+                 : "r"((u32)pred), "r"(bar_id), "r"(TPG)
+                 : "memory");
+    return r != 0;
+}
+
 __device__ __forceinline__ void issue_slab(u64 *slab, const u64 *src, u64 *mbar)
 {
     mbar_expect_tx(mbar, (u32)SLAB_BYTES);
@@ -414,15 +428,17 @@ __global__ void __launch_bounds__(G * 256, 1)
     u64 *slab = reinterpret_cast<u64 *>(smem_raw);
     u64 *tws = slab + SLAB_WORDS;
     u64 *bufs = tws + 4096;
-    u64 *mbar = bufs + G * 2 * POLY_WORDS;
-    u32 *lwes = reinterpret_cast<u32 *>(mbar + 2);
+    u64 *mbar = bufs + G * 4 * POLY_WORDS;
+    u32 *slab_done = reinterpret_cast<u32 *>(mbar + 1);  // groups that finished the current slab
+    u32 *failed = slab_done + 1;
     const int g = threadIdx.x >> 8, t = threadIdx.x & 255, bar = 1 + g;
-    u64 *buf = bufs + g * 2 * POLY_WORDS;
-    u32 *my_lwe = lwes + g * (n + 1);
+    // two staging buffers per ciphertext group, swapped every step (see forward2)
+    u64 *bp = bufs + g * 4 * POLY_WORDS, *bq = bp + 2 * POLY_WORDS;
 
     for (int i = threadIdx.x; i < 4096; i += G * TPG) tws[i] = tw[i];
     if (threadIdx.x == 0) {
         mbar_init(mbar, 1);
+        *failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -433,7 +449,7 @@ __global__ void __launch_bounds__(G * 256, 1)
         const u32 cidx = grp * G + g;
         const bool active = cidx < B;
         const u32 ct = active ? cidx : B - 1;
-        for (u32 i = t; i <= n; i += TPG) my_lwe[i] = lwe2N[(size_t)ct * (n + 1) + i];
+        const u32 *my_lwe = lwe2N + (size_t)ct * (n + 1);  // read in place; every thread of the group loads the same word
         u32 lid = lut_id[ct];
         if (lid >= nlut) lid = 0;  // host validates ids; keep the read in bounds regardless
         const u64 *lut = luts + (size_t)lid * 2 * N;
@@ -442,16 +458,27 @@ __global__ void __launch_bounds__(G * 256, 1)
         for (int q = 0; q < 2; q++)
 #pragma unroll
             for (int e = 0; e < 8; e++) acc[q][e] = lut[q * N + ntt::coef_index(t, e)];
-        if (threadIdx.x == 0) issue_slab(slab, bsk, mbar);
+        if (threadIdx.x == 0) {
+            *slab_done = 0;
+            issue_slab(slab, bsk, mbar);
+        }
         __syncthreads();
 
+        // The G groups run their steps independently (so one group's NTT overlaps
+        // another's BSK multiply); they share only the slab, which the last group
+        // to finish a step's multiply refills.  A group that times out on the slab
+        // stops; the others then time out too (no refill comes) and all meet at
+        // the block barrier after the loop.
+        bool ok = true;
+        u32 a_next = my_lwe[0];
         for (u32 i = 0; i < n; i++) {
-            const u32 a = my_lwe[i];
+            const u32 a = a_next;
+            a_next = my_lwe[i + 1];  // i + 1 <= n: the body word at the end
             // feed: diff = X^a ACC - ACC, decomposed into Z_p
 #pragma unroll
             for (int q = 0; q < 2; q++)
 #pragma unroll
-                for (int e = 0; e < 8; e++) buf[q * POLY_WORDS + ntt::coef_index(t, e)] = acc[q][e];
+                for (int e = 0; e < 8; e++) bp[q * POLY_WORDS + ntt::coef_index(t, e)] = acc[q][e];
             ntt::group_sync(bar);
             u64 x[2][8];
 #pragma unroll
@@ -460,14 +487,16 @@ __global__ void __launch_bounds__(G * 256, 1)
                 for (int e = 0; e < 8; e++) {
                     const u32 j = ntt::coef_index(t, e);
                     const u32 src = (j + TWO_N - a) & (TWO_N - 1);
-                    u64 v = buf[q * POLY_WORDS + (src & (N - 1))];
+                    u64 v = bp[q * POLY_WORDS + (src & (N - 1))];
                     if (src >= (u32)N) v = 0ull - v;
                     x[q][e] = gl::decomp_to_p<BW>(v - acc[q][e]);
                 }
-            ntt::group_sync(bar);
-            ntt::forward<2>(x, buf, tws, t, bar);
+            // A1 writes bq (last read by the previous step's A1^-1, which every
+            // thread finished before the barrier above); A2 writes bp (read
+            // above, before A1's barrier)
+            ntt::forward2<2>(x, bq, bp, tws, t, bar);
             // BSK multiply-accumulate in the evaluation domain
-            const bool ok = mbar_wait(mbar, phase);
+            ok = mbar_wait(mbar, phase);
             phase ^= 1;
             u64 r[2][8];
 #pragma unroll
@@ -477,17 +506,32 @@ __global__ void __launch_bounds__(G * 256, 1)
                 r[0][p] = gl::mul_add2(x[0][p], b00, x[1][p], b10);
                 r[1][p] = gl::mul_add2(x[0][p], b01, x[1][p], b11);
             }
-            if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) atomicExch(err, 1u);
-                return;
+            if (group_sync_or(bar, !ok)) {
+                ok = false;
+                break;
             }
-            if (threadIdx.x == 0 && i + 1 < n) issue_slab(slab, bsk + (size_t)(i + 1) * SLAB_WORDS, mbar);
-            ntt::inverse<2>(r, buf, tws + 2048, t, bar);
+            if (t == 0) {
+                __threadfence_block();
+                const u32 done = atomicAdd(slab_done, 1u) + 1;
+                if (done == (u32)G * (i + 1) && i + 1 < n) {
+                    // every group has read slab i: reuse the buffer for slab i+1
+                    __threadfence_block();
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    issue_slab(slab, bsk + (size_t)(i + 1) * SLAB_WORDS, mbar);
+                }
+            }
+            // C2^-1 writes bp (last read by C1, before C1's barrier), C1^-1
+            // writes bq (last read by C2, before the block barrier); A1^-1 reads bp
+            ntt::inverse2<2>(r, bp, bq, tws + 2048, t, bar);
 #pragma unroll
             for (int q = 0; q < 2; q++)
 #pragma unroll
                 for (int e = 0; e < 8; e++) acc[q][e] += gl::modsw_p_to_q(gl::canon(r[q][e]));
-            ntt::group_sync(bar);
+            // A1^-1 is still reading bp: the next step starts in bq (last read by
+            // A2^-1, before the barrier after its writes)
+            u64 *tmp = bp;
+            bp = bq;
+            bq = tmp;
         }
 
         // sample extract of coefficient 0 of X^{-b} ACC.  Many-LUT (mlk = 2, 4, 8
@@ -497,36 +541,44 @@ __global__ void __launch_bounds__(G * 256, 1)
 #pragma unroll
         for (int q = 0; q < 2; q++)
 #pragma unroll
-            for (int e = 0; e < 8; e++) buf[q * POLY_WORDS + ntt::coef_index(t, e)] = acc[q][e];
+            for (int e = 0; e < 8; e++) bp[q * POLY_WORDS + ntt::coef_index(t, e)] = acc[q][e];
         ntt::group_sync(bar);
-        if (active) {
+        if (!ok) {
+            if (t == 0) {
+                atomicExch(failed, 1u);
+                atomicExch(err, 1u);
+            }
+        } else if (active) {
             const size_t row0 = dst_idx ? dst_idx[cidx] : (size_t)cidx * mlk;
+            const u32 body = my_lwe[n];
             for (u32 m = 0; m < mlk; m++) {
-                const u32 b = (my_lwe[n] + m * (N / mlk)) & (TWO_N - 1);
+                const u32 b = (body + m * (N / mlk)) & (TWO_N - 1);
                 u64 *o = out + (row0 + m) * (N + 1);
 #pragma unroll
                 for (int r = 0; r < 8; r++) {
                     const u32 oi = t + 256 * r;
                     const u32 j = oi == 0 ? 0 : N - oi;
                     const u32 src = (j + b) & (TWO_N - 1);
-                    u64 v = buf[src & (N - 1)];
+                    u64 v = bp[src & (N - 1)];
                     if (src >= (u32)N) v = 0ull - v;
                     o[oi] = oi == 0 ? v : 0ull - v;
                 }
                 if (t == 0) {
-                    u64 v = buf[POLY_WORDS + (b & (N - 1))];
+                    u64 v = bp[POLY_WORDS + (b & (N - 1))];
                     o[N] = b >= (u32)N ? 0ull - v : v;
                 }
             }
         }
         __syncthreads();
+        if (*failed) return;  // read by every thread after the barrier: uniform
     }
 }
 
 size_t br_smem_bytes(const BrConfig &cfg, uint32_t n)
 {
     const int G = cfg.cts_per_cta;
-    return (size_t)(SLAB_WORDS + 4096 + G * 2 * POLY_WORDS + 2) * 8 + (size_t)G * (n + 1) * 4;
+    (void)n;
+    return (size_t)(SLAB_WORDS + 4096 + G * 4 * POLY_WORDS + 2) * 8;
 }
 
 template <int G, int BW>

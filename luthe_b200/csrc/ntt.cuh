@@ -339,6 +339,149 @@ __device__ __forceinline__ void inverse(u64 (&x)[NP][8], u64 *buf, const u64 *tw
     }
 }
 
+// Double-buffered forms: the three exchanges of a transform alternate between
+// two staging buffers (b0, b1: NP * POLY_WORDS words each), so each exchange
+// needs one barrier (after its writes) instead of two -- a buffer is rewritten
+// only after the barrier that follows the last read of it.
+// forward2: A1 writes b0, A2 writes b1, C1 writes b0.  The caller guarantees
+// that nobody still reads b0 or b1 when it is called (a barrier after their
+// last reads), and may reuse b1 once the next barrier has passed (C2 reads b0).
+template <int NP>
+__device__ __forceinline__ void forward2(u64 (&x)[NP][8], u64 *b0, u64 *b1, const u64 *tw_fwd, int t, int bar_id)
+{
+    {
+        const int j1a = t >> 6, j2 = t & 63;
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            ct8_neg(x[q]);
+            tw_a1_rt<1>(x[q], j1a);
+            u64 *b = b0 + q * POLY_WORDS;
+#pragma unroll
+            for (int p = 0; p < 8; p++) b[(j1a * 8 + brv3(p)) * 64 + j2] = x[q][p];
+        }
+    }
+    group_sync(bar_id);
+    {
+        const int kp = t >> 6, j2 = t & 63;
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            const u64 *b = b0 + q * POLY_WORDS;
+#pragma unroll
+            for (int c = 0; c < 2; c++)
+#pragma unroll
+                for (int j1a = 0; j1a < 4; j1a++) x[q][c * 4 + j1a] = b[(j1a * 8 + kp + 4 * c) * 64 + j2];
+        }
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            dif4(x[q]);
+            dif4(x[q] + 4);
+            u64 *b = b1 + q * POLY_WORDS;
+#pragma unroll
+            for (int s = 0; s < 8; s++) {
+                u64 v = gl::mul(x[q][s], tw_fwd[s * TPG + t]);
+                b[(kp + 4 * (s >> 2) + 8 * brv2(s & 3)) * 65 + j2] = v;
+            }
+        }
+    }
+    group_sync(bar_id);
+    {
+        const int j2a = t >> 5, k1 = t & 31;
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            const u64 *b = b1 + q * POLY_WORDS;
+#pragma unroll
+            for (int j2b = 0; j2b < 8; j2b++) x[q][j2b] = b[k1 * 65 + j2a + 8 * j2b];
+        }
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            dif8(x[q]);
+            tw_c1_rt<1>(x[q], j2a);
+            u64 *b = b0 + q * POLY_WORDS;
+#pragma unroll
+            for (int p = 0; p < 8; p++) b[(j2a * 8 + brv3(p)) * 32 + k1] = x[q][p];
+        }
+    }
+    group_sync(bar_id);
+    {
+        const int k2b = t >> 5, k1 = t & 31;
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            const u64 *b = b0 + q * POLY_WORDS;
+#pragma unroll
+            for (int j2a = 0; j2a < 8; j2a++) x[q][j2a] = b[(j2a * 8 + k2b) * 32 + k1];
+            dif8(x[q]);
+        }
+    }
+}
+
+// inverse2: C2^-1 writes b0, C1^-1 writes b1, A2^-1 writes b0; A1^-1 reads b0.
+// Same contract as forward2.
+template <int NP>
+__device__ __forceinline__ void inverse2(u64 (&x)[NP][8], u64 *b0, u64 *b1, const u64 *tw_inv, int t, int bar_id)
+{
+    {
+        const int k2b = t >> 5, k1 = t & 31;
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            dit8_inv(x[q]);
+            u64 *b = b0 + q * POLY_WORDS;
+#pragma unroll
+            for (int j2a = 0; j2a < 8; j2a++) b[(j2a * 8 + k2b) * 32 + k1] = x[q][j2a];
+        }
+    }
+    group_sync(bar_id);
+    {
+        const int j2a = t >> 5, k1 = t & 31;
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            const u64 *b = b0 + q * POLY_WORDS;
+#pragma unroll
+            for (int p = 0; p < 8; p++) x[q][p] = b[(j2a * 8 + brv3(p)) * 32 + k1];
+        }
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            tw_c1_rt<-1>(x[q], j2a);
+            dit8_inv(x[q]);
+            u64 *b = b1 + q * POLY_WORDS;
+#pragma unroll
+            for (int j2b = 0; j2b < 8; j2b++) b[k1 * 65 + j2a + 8 * j2b] = x[q][j2b];
+        }
+    }
+    group_sync(bar_id);
+    {
+        const int kp = t >> 6, j2 = t & 63;
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            const u64 *b = b1 + q * POLY_WORDS;
+#pragma unroll
+            for (int s = 0; s < 8; s++)
+                x[q][s] = gl::mul(b[(kp + 4 * (s >> 2) + 8 * brv2(s & 3)) * 65 + j2], tw_inv[s * TPG + t]);
+        }
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            dit4_inv(x[q]);
+            dit4_inv(x[q] + 4);
+            u64 *b = b0 + q * POLY_WORDS;
+#pragma unroll
+            for (int c = 0; c < 2; c++)
+#pragma unroll
+                for (int j1a = 0; j1a < 4; j1a++) b[(j1a * 8 + kp + 4 * c) * 64 + j2] = x[q][c * 4 + j1a];
+        }
+    }
+    group_sync(bar_id);
+    {
+        const int j1a = t >> 6, j2 = t & 63;
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            const u64 *b = b0 + q * POLY_WORDS;
+#pragma unroll
+            for (int p = 0; p < 8; p++) x[q][p] = b[(j1a * 8 + brv3(p)) * 64 + j2];
+            tw_a1_rt<-1>(x[q], j1a);
+            gs8_neg_inv(x[q]);
+        }
+    }
+}
+
 // Coefficient index held by thread t in slot e of the coefficient layout.
 __host__ __device__ inline int coef_index(int t, int e) { return 64 * (t >> 6) + 256 * e + (t & 63); }
 // Evaluation index k held by thread t in slot p of the evaluation layout.
