@@ -94,7 +94,35 @@ __device__ __forceinline__ u64 reduce96(u64 lo, u32 h0)
     return r;
 }
 
-__device__ __forceinline__ u64 mul(u64 a, u64 b) { return reduce128(a * b, __umul64hi(a, b)); }
+// a * b as 128 bits (hi:lo): the four 32 x 32 partial products and their
+// carries as one multiply-add chain (mad.lo/madc.hi with carry flags), which
+// keeps the whole product on the multiply pipe.
+__device__ __forceinline__ void mul_wide(u64 a, u64 b, u64 &lo, u64 &hi)
+{
+    asm("{\n\t.reg .u32 a0, a1, b0, b1, r0, r1, r2, r3;\n\t"
+        "mov.b64 {a0, a1}, %2;\n\t"
+        "mov.b64 {b0, b1}, %3;\n\t"
+        "mul.lo.u32 r0, a0, b0;\n\t"
+        "mul.hi.u32 r1, a0, b0;\n\t"
+        "mad.lo.cc.u32 r1, a0, b1, r1;\n\t"
+        "madc.hi.u32 r2, a0, b1, 0;\n\t"
+        "mad.lo.cc.u32 r1, a1, b0, r1;\n\t"
+        "madc.hi.cc.u32 r2, a1, b0, r2;\n\t"
+        "madc.hi.u32 r3, a1, b1, 0;\n\t"
+        "mad.lo.cc.u32 r2, a1, b1, r2;\n\t"
+        "addc.u32 r3, r3, 0;\n\t"
+        "mov.b64 %0, {r0, r1};\n\t"
+        "mov.b64 %1, {r2, r3};\n\t}"
+        : "=l"(lo), "=l"(hi)
+        : "l"(a), "l"(b));
+}
+
+__device__ __forceinline__ u64 mul(u64 a, u64 b)
+{
+    u64 lo, hi;
+    mul_wide(a, b, lo, hi);
+    return reduce128(lo, hi);
+}
 
 __device__ __forceinline__ u64 canon(u64 a) { return a >= P ? a - P : a; }
 
@@ -102,20 +130,57 @@ __device__ __forceinline__ u64 neg(u64 a) { return sub(0ull, a); }
 
 __host__ __device__ constexpr int mod192(int s) { return ((s % 192) + 192) % 192; }
 
-// x * 2^S for a compile-time S (any sign; 2^192 == 1).
+// x * 2^-k for 0 < k < 32 and any x < 2^64: (x + m p) / 2^k with
+// m = -x mod 2^k.  p = 1 (mod 2^32) makes x + m p divisible by 2^k, and the
+// quotient is below 2^64 (it is below p + 2^(32-k)), so one exact division
+// replaces the three folds that x * 2^(96-k) would take.
+__device__ __forceinline__ u64 div2k(u64 x, u32 k)
+{
+    const u32 m = (0u - (u32)x) & ((1u << k) - 1u);
+    u64 r;
+    asm("{\n\t.reg .u32 t0, t1, c, top, r0, r1;\n\t"
+        "mov.b64 {t0, t1}, %1;\n\t"
+        "add.cc.u32 t0, t0, %2;\n\t"   // x + m
+        "addc.cc.u32 t1, t1, 0;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "sub.cc.u32 t1, t1, %2;\n\t"   // - m 2^32
+        "subc.u32 top, %2, 0;\n\t"     // + m 2^64, less the borrow
+        "add.u32 top, top, c;\n\t"
+        "shf.r.wrap.b32 r0, t0, t1, %3;\n\t"
+        "shf.r.wrap.b32 r1, t1, top, %3;\n\t"
+        "mov.b64 %0, {r0, r1};\n\t}"
+        : "=l"(r)
+        : "l"(x), "r"(m), "r"(k));
+    return r;
+}
+
+// x * 2^S for a compile-time S (any sign; 2^192 == 1) is (-1)^shl_neg(S) *
+// shl_abs<S>(x): with s = S mod 96, shifts up to 32 are one 96-bit fold, up
+// to 64 two, and above 64 the division x 2^s = -x / 2^(96-s).  Butterflies
+// absorb the sign by swapping their add and subtract.
+__host__ __device__ constexpr bool shl_neg(int S)
+{
+    return (mod192(S) >= 96) != (mod192(S) % 96 > 64);
+}
+template <int S>
+__device__ __forceinline__ u64 shl_abs(u64 x)
+{
+    constexpr int s = mod192(S) % 96;
+    if constexpr (s == 0) {
+        return x;
+    } else if constexpr (s <= 32) {
+        return reduce96(x << s, (u32)(x >> (64 - s)));
+    } else if constexpr (s > 64) {
+        return div2k(x, 96 - s);
+    } else {
+        return shl_abs<32>(shl_abs<s - 32>(x));  // two 96-bit folds beat one 128-bit fold
+    }
+}
 template <int S>
 __device__ __forceinline__ u64 shl(u64 x)
 {
-    constexpr int s = mod192(S);
-    if constexpr (s == 0) {
-        return x;
-    } else if constexpr (s >= 96) {
-        return neg(shl<s - 96>(x));  // 2^96 == -1
-    } else if constexpr (s <= 32) {
-        return reduce96(x << s, (u32)(x >> (64 - s)));
-    } else {
-        return shl<32>(shl<s - 32>(x));  // two 96-bit folds beat one 128-bit fold
-    }
+    if constexpr (shl_neg(S)) return neg(shl_abs<S>(x));
+    else return shl_abs<S>(x);
 }
 
 // x * 2^s for a runtime s in [0, 192) that is uniform across the warp: one
@@ -123,18 +188,18 @@ __device__ __forceinline__ u64 shl(u64 x)
 // never diverge.
 __device__ __forceinline__ u64 shl_rt(u64 x, u32 s)
 {
-    const bool negate = s >= 96;
+    bool negate = s >= 96;
     if (negate) s -= 96;
-    if (s > 32) {
-        const u32 s1 = s > 64 ? 32 : s - 32;  // first fold: s1 in [1, 32]
-        x = reduce96(x << s1, (u32)(x >> (64 - s1)));
-        s -= s1;
+    if (s > 64) {
+        x = div2k(x, 96 - s);  // x 2^s = -x / 2^(96-s)
+        negate = !negate;
+    } else {
         if (s > 32) {
             x = reduce96(x << 32, (u32)(x >> 32));
             s -= 32;
         }
+        if (s) x = reduce96(x << s, (u32)(x >> (64 - s)));
     }
-    if (s) x = reduce96(x << s, (u32)(x >> (64 - s)));
     return negate ? neg(x) : x;
 }
 
@@ -142,9 +207,10 @@ __device__ __forceinline__ u64 shl_rt(u64 x, u32 s)
 // a carry out of bit 128 is worth 2^128 == -2^32 (mod p).
 __device__ __forceinline__ u64 mul_add2(u64 a, u64 b, u64 c, u64 d)
 {
-    u64 lo, hi;
+    u64 lo, hi, l1, h1, l2, h2;
     u32 c2;
-    const u64 l1 = a * b, h1 = __umul64hi(a, b), l2 = c * d, h2 = __umul64hi(c, d);
+    mul_wide(a, b, l1, h1);
+    mul_wide(c, d, l2, h2);
     asm("add.cc.u64 %0, %3, %4;\n\t"
         "addc.cc.u64 %1, %5, %6;\n\t"
         "addc.u32 %2, 0, 0;"
@@ -157,15 +223,13 @@ __device__ __forceinline__ u64 mul_add2(u64 a, u64 b, u64 c, u64 d)
 template <int S>
 __device__ __forceinline__ void ct_bf(u64 &u, u64 &v)
 {
-    constexpr int s = mod192(S);
-    if constexpr (s >= 96) {
-        u64 t = shl<s - 96>(v);
-        u64 a = sub(u, t);
+    const u64 t = shl_abs<S>(v);
+    if constexpr (shl_neg(S)) {
+        const u64 a = sub(u, t);
         v = add(u, t);
         u = a;
     } else {
-        u64 t = shl<s>(v);
-        u64 a = add(u, t);
+        const u64 a = add(u, t);
         v = sub(u, t);
         u = a;
     }
@@ -175,29 +239,21 @@ __device__ __forceinline__ void ct_bf(u64 &u, u64 &v)
 template <int S>
 __device__ __forceinline__ void gs_bf(u64 &u, u64 &v)
 {
-    constexpr int s = mod192(S);
-    if constexpr (s >= 96) {
-        u64 a = add(u, v);
-        v = shl<s - 96>(sub(v, u));
-        u = a;
-    } else {
-        u64 a = add(u, v);
-        v = shl<s>(sub(u, v));
-        u = a;
-    }
+    const u64 a = add(u, v);
+    v = shl_abs<S>(shl_neg(S) ? sub(v, u) : sub(u, v));
+    u = a;
 }
 
 // p -> 2^64 modulus switch of a canonical residue a:
 //   z = ((a * CST) >> 96) + bit95(a * CST),  CST = floor(2^160 / p) = 2^96 + 2^64 - 2
 // (hw/common_lib/.../mod_switch_to_2powerN.sv:62-64,132-134 with
-//  MOD_Q_W = 64, PRECISION_W = 96).
+//  MOD_Q_W = 64, PRECISION_W = 96).  a * CST = a 2^96 + (a 2^64 - 2a), and the
+// 64-bit word above 2^64 of a 2^64 - 2a is hx = a - [a > 0] - [a > 2^63], so
+// z = a + round(hx / 2^32) mod 2^64 -- no multiply.
 __device__ __forceinline__ u64 modsw_p_to_q(u64 a)
 {
-    const u64 cst_lo = 0xFFFFFFFFFFFFFFFEull;  // CST mod 2^64; CST >> 64 = 2^32
-    u64 ph = __umul64hi(a, cst_lo);
-    u64 m = ph + (a << 32);
-    u64 top = (a >> 32) + (m < ph ? 1ull : 0ull);
-    return (top << 32) + (m >> 32) + ((m >> 31) & 1ull);
+    const u64 hx = a - (a != 0 ? 1ull : 0ull) - (a > 0x8000000000000000ull ? 1ull : 0ull);
+    return a + ((hx + 0x80000000ull) >> 32);
 }
 
 // Balanced decomposition, base 2^23, one level, of a 64-bit torus value,
