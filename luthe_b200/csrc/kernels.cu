@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(G * 256, 1)
     u32 *slab_done = reinterpret_cast<u32 *>(mbar + 1);  // groups that finished the current slab
     u32 *failed = slab_done + 1;
     const int g = threadIdx.x >> 8, t = threadIdx.x & 255, bar = 1 + g;
-    // two staging buffers per ciphertext group, swapped every step (see forward2)
+    // two staging buffers per ciphertext group (fixed roles, see the step below)
     u64 *bp = bufs + g * 4 * POLY_WORDS, *bq = bp + 2 * POLY_WORDS;
 
     for (int i = threadIdx.x; i < 4096; i += G * TPG) tws[i] = tw[i];
@@ -453,11 +453,17 @@ __global__ void __launch_bounds__(G * 256, 1)
         u32 lid = lut_id[ct];
         if (lid >= nlut) lid = 0;  // host validates ids; keep the read in bounds regardless
         const u64 *lut = luts + (size_t)lid * 2 * N;
+        // ACC: registers (coefficient layout, 16 coefficients per thread), copied
+        // to the thread's own slots of bp at the start of every step
         u64 acc[2][8];
 #pragma unroll
         for (int q = 0; q < 2; q++)
 #pragma unroll
-            for (int e = 0; e < 8; e++) acc[q][e] = lut[q * N + ntt::coef_index(t, e)];
+            for (int e = 0; e < 8; e++) {
+                const int j = ntt::coef_index(t, e);
+                acc[q][e] = lut[q * N + j];
+                bp[q * POLY_WORDS + j] = acc[q][e];
+            }
         if (threadIdx.x == 0) {
             *slab_done = 0;
             issue_slab(slab, bsk, mbar);
@@ -469,42 +475,61 @@ __global__ void __launch_bounds__(G * 256, 1)
         // to finish a step's multiply refills.  A group that times out on the slab
         // stops; the others then time out too (no refill comes) and all meet at
         // the block barrier after the loop.
+        //
+        // One step, buffer by buffer (every write follows the barrier after the
+        // last read of what it overwrites; "own" slots are read and written only
+        // by the thread that owns them):
+        //   ACC (bp, own) --barrier--> rotate+decompose+A1 -> bq --> A2 -> bp
+        //   --> C1 -> bq --> C2 -> bp (own) ; BSK MAC bp (own) -> bp (own)
+        //   --barrier--> C2^-1 -> bq --> C1^-1 -> bp --> A2^-1 -> bq --> A1^-1
+        //   -> bp (own) ; accumulate into ACC, ACC -> bp (own)
+        // (the own slots of thread t are t + 256 e in both the coefficient and
+        // the evaluation layout)
+        // Passes run one polynomial at a time (rolled loops): one copy of each
+        // pass's code keeps the step inside the instruction cache.
         bool ok = true;
         u32 a_next = my_lwe[0];
         for (u32 i = 0; i < n; i++) {
             const u32 a = a_next;
             a_next = my_lwe[i + 1];  // i + 1 <= n: the body word at the end
-            // feed: diff = X^a ACC - ACC, decomposed into Z_p
-#pragma unroll
-            for (int q = 0; q < 2; q++)
-#pragma unroll
-                for (int e = 0; e < 8; e++) bp[q * POLY_WORDS + ntt::coef_index(t, e)] = acc[q][e];
             ntt::group_sync(bar);
-            u64 x[2][8];
-#pragma unroll
-            for (int q = 0; q < 2; q++)
+            // feed: diff = X^a ACC - ACC, decomposed into Z_p, then A1
+#pragma unroll 1
+            for (int q = 0; q < 2; q++) {
+                const u64 *accq = bp + q * POLY_WORDS;
+                u64 y[8];
 #pragma unroll
                 for (int e = 0; e < 8; e++) {
                     const u32 j = ntt::coef_index(t, e);
                     const u32 src = (j + TWO_N - a) & (TWO_N - 1);
-                    u64 v = bp[q * POLY_WORDS + (src & (N - 1))];
+                    u64 v = accq[src & (N - 1)];
                     if (src >= (u32)N) v = 0ull - v;
-                    x[q][e] = gl::decomp_to_p<BW>(v - acc[q][e]);
+                    y[e] = gl::decomp_to_p<BW>(v - accq[j]);
                 }
-            // A1 writes bq (last read by the previous step's A1^-1, which every
-            // thread finished before the barrier above); A2 writes bp (read
-            // above, before A1's barrier)
-            ntt::forward2<2>(x, bq, bp, tws, t, bar);
+                ntt::a1_fwd(y, bq + q * POLY_WORDS, t);
+            }
+            ntt::group_sync(bar);
+            ntt::a2_fwd<2>(bq, bp, tws, t);
+            ntt::group_sync(bar);
+            ntt::c1_fwd<2>(bp, bq, t);
+            ntt::group_sync(bar);
+#pragma unroll 1
+            for (int q = 0; q < 2; q++) {
+                u64 y[8];
+                ntt::c2_fwd(bq + q * POLY_WORDS, y, t);
+#pragma unroll
+                for (int p = 0; p < 8; p++) bp[q * POLY_WORDS + p * TPG + t] = y[p];  // own slots
+            }
             // BSK multiply-accumulate in the evaluation domain
             ok = mbar_wait(mbar, phase);
             phase ^= 1;
-            u64 r[2][8];
 #pragma unroll
             for (int p = 0; p < 8; p++) {
                 const u64 *sb = slab + p * 4 * TPG + t;
                 const u64 b00 = sb[0], b01 = sb[TPG], b10 = sb[2 * TPG], b11 = sb[3 * TPG];
-                r[0][p] = gl::mul_add2(x[0][p], b00, x[1][p], b10);
-                r[1][p] = gl::mul_add2(x[0][p], b01, x[1][p], b11);
+                const u64 x0 = bp[p * TPG + t], x1 = bp[POLY_WORDS + p * TPG + t];
+                bp[p * TPG + t] = gl::mul_add2(x0, b00, x1, b10);
+                bp[POLY_WORDS + p * TPG + t] = gl::mul_add2(x0, b01, x1, b11);
             }
             if (group_sync_or(bar, !ok)) {
                 ok = false;
@@ -520,29 +545,41 @@ __global__ void __launch_bounds__(G * 256, 1)
                     issue_slab(slab, bsk + (size_t)(i + 1) * SLAB_WORDS, mbar);
                 }
             }
-            // C2^-1 writes bp (last read by C1, before C1's barrier), C1^-1
-            // writes bq (last read by C2, before the block barrier); A1^-1 reads bp
-            ntt::inverse2<2>(r, bp, bq, tws + 2048, t, bar);
+#pragma unroll 1
+            for (int q = 0; q < 2; q++) {
+                u64 y[8];
+#pragma unroll
+                for (int p = 0; p < 8; p++) y[p] = bp[q * POLY_WORDS + p * TPG + t];
+                ntt::c2_inv(y, bq + q * POLY_WORDS, t);
+            }
+            ntt::group_sync(bar);
+            ntt::c1_inv<2>(bq, bp, t);
+            ntt::group_sync(bar);
+            ntt::a2_inv<2>(bp, bq, tws + 2048, t);
+            ntt::group_sync(bar);
+#pragma unroll 1
+            for (int q = 0; q < 2; q++) {
+                u64 y[8];
+                ntt::a1_inv(bq + q * POLY_WORDS, y, t);
+#pragma unroll
+                for (int e = 0; e < 8; e++) bp[q * POLY_WORDS + ntt::coef_index(t, e)] = y[e];  // own slots
+            }
+            // p -> 2^64 switch, accumulate, and ACC to the own slots for the next step
 #pragma unroll
             for (int q = 0; q < 2; q++)
 #pragma unroll
-                for (int e = 0; e < 8; e++) acc[q][e] += gl::modsw_p_to_q(gl::canon(r[q][e]));
-            // A1^-1 is still reading bp: the next step starts in bq (last read by
-            // A2^-1, before the barrier after its writes)
-            u64 *tmp = bp;
-            bp = bq;
-            bq = tmp;
+                for (int e = 0; e < 8; e++) {
+                    u64 *slot = bp + q * POLY_WORDS + ntt::coef_index(t, e);
+                    acc[q][e] += gl::modsw_p_to_q(gl::canon(*slot));
+                    *slot = acc[q][e];
+                }
         }
 
         // sample extract of coefficient 0 of X^{-b} ACC.  Many-LUT (mlk = 2, 4, 8
         // functions packed in one LUT, docs/dop.md:113-121): output m extracts
         // coefficient m*N/mlk, i.e. coefficient 0 of X^{-(b + m N/mlk)} ACC,
         // into consecutive output rows.
-#pragma unroll
-        for (int q = 0; q < 2; q++)
-#pragma unroll
-            for (int e = 0; e < 8; e++) bp[q * POLY_WORDS + ntt::coef_index(t, e)] = acc[q][e];
-        ntt::group_sync(bar);
+        ntt::group_sync(bar);  // ACC (bp) complete
         if (!ok) {
             if (t == 0) {
                 atomicExch(failed, 1u);

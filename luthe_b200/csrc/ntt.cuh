@@ -339,147 +339,122 @@ __device__ __forceinline__ void inverse(u64 (&x)[NP][8], u64 *buf, const u64 *tw
     }
 }
 
-// Double-buffered forms: the three exchanges of a transform alternate between
-// two staging buffers (b0, b1: NP * POLY_WORDS words each), so each exchange
-// needs one barrier (after its writes) instead of two -- a buffer is rewritten
-// only after the barrier that follows the last read of it.
-// forward2: A1 writes b0, A2 writes b1, C1 writes b0.  The caller guarantees
-// that nobody still reads b0 or b1 when it is called (a barrier after their
-// last reads), and may reuse b1 once the next barrier has passed (C2 reads b0).
-template <int NP>
-__device__ __forceinline__ void forward2(u64 (&x)[NP][8], u64 *b0, u64 *b1, const u64 *tw_fwd, int t, int bar_id)
+// Single-pass building blocks for callers that run a transform one polynomial
+// at a time (a rolled loop: one copy of the pass code for every polynomial,
+// which keeps a whole blind-rotation step inside the instruction cache).  Each
+// reads one staging buffer and writes another; barriers are the caller's.
+// Layouts as in forward/inverse above.
+
+// A1 of one polynomial held in registers (coefficient layout) -> dst
+__device__ __forceinline__ void a1_fwd(u64 *y, u64 *dst, int t)
 {
-    {
-        const int j1a = t >> 6, j2 = t & 63;
+    const int j1a = t >> 6, j2 = t & 63;
+    ct8_neg(y);
+    tw_a1_rt<1>(y, j1a);
 #pragma unroll
-        for (int q = 0; q < NP; q++) {
-            ct8_neg(x[q]);
-            tw_a1_rt<1>(x[q], j1a);
-            u64 *b = b0 + q * POLY_WORDS;
+    for (int p = 0; p < 8; p++) dst[(j1a * 8 + brv3(p)) * 64 + j2] = y[p];
+}
+// A2 + B of NP polynomials: src (A1 layout) -> dst (padded k1 layout)
+template <int NP>
+__device__ __forceinline__ void a2_fwd(const u64 *src, u64 *dst, const u64 *tw_fwd, int t)
+{
+    const int kp = t >> 6, j2 = t & 63;
+#pragma unroll 1
+    for (int q = 0; q < NP; q++) {
+        const u64 *b = src + q * POLY_WORDS;
+        u64 y[8];
 #pragma unroll
-            for (int p = 0; p < 8; p++) b[(j1a * 8 + brv3(p)) * 64 + j2] = x[q][p];
-        }
-    }
-    group_sync(bar_id);
-    {
-        const int kp = t >> 6, j2 = t & 63;
+        for (int c = 0; c < 2; c++)
 #pragma unroll
-        for (int q = 0; q < NP; q++) {
-            const u64 *b = b0 + q * POLY_WORDS;
+            for (int j1a = 0; j1a < 4; j1a++) y[c * 4 + j1a] = b[(j1a * 8 + kp + 4 * c) * 64 + j2];
+        dif4(y);
+        dif4(y + 4);
+        u64 *o = dst + q * POLY_WORDS;
 #pragma unroll
-            for (int c = 0; c < 2; c++)
-#pragma unroll
-                for (int j1a = 0; j1a < 4; j1a++) x[q][c * 4 + j1a] = b[(j1a * 8 + kp + 4 * c) * 64 + j2];
-        }
-#pragma unroll
-        for (int q = 0; q < NP; q++) {
-            dif4(x[q]);
-            dif4(x[q] + 4);
-            u64 *b = b1 + q * POLY_WORDS;
-#pragma unroll
-            for (int s = 0; s < 8; s++) {
-                u64 v = gl::mul(x[q][s], tw_fwd[s * TPG + t]);
-                b[(kp + 4 * (s >> 2) + 8 * brv2(s & 3)) * 65 + j2] = v;
-            }
-        }
-    }
-    group_sync(bar_id);
-    {
-        const int j2a = t >> 5, k1 = t & 31;
-#pragma unroll
-        for (int q = 0; q < NP; q++) {
-            const u64 *b = b1 + q * POLY_WORDS;
-#pragma unroll
-            for (int j2b = 0; j2b < 8; j2b++) x[q][j2b] = b[k1 * 65 + j2a + 8 * j2b];
-        }
-#pragma unroll
-        for (int q = 0; q < NP; q++) {
-            dif8(x[q]);
-            tw_c1_rt<1>(x[q], j2a);
-            u64 *b = b0 + q * POLY_WORDS;
-#pragma unroll
-            for (int p = 0; p < 8; p++) b[(j2a * 8 + brv3(p)) * 32 + k1] = x[q][p];
-        }
-    }
-    group_sync(bar_id);
-    {
-        const int k2b = t >> 5, k1 = t & 31;
-#pragma unroll
-        for (int q = 0; q < NP; q++) {
-            const u64 *b = b0 + q * POLY_WORDS;
-#pragma unroll
-            for (int j2a = 0; j2a < 8; j2a++) x[q][j2a] = b[(j2a * 8 + k2b) * 32 + k1];
-            dif8(x[q]);
-        }
+        for (int s = 0; s < 8; s++) o[(kp + 4 * (s >> 2) + 8 * brv2(s & 3)) * 65 + j2] = gl::mul(y[s], tw_fwd[s * TPG + t]);
     }
 }
-
-// inverse2: C2^-1 writes b0, C1^-1 writes b1, A2^-1 writes b0; A1^-1 reads b0.
-// Same contract as forward2.
+// C1 of NP polynomials: src (padded k1 layout) -> dst (C1 layout)
 template <int NP>
-__device__ __forceinline__ void inverse2(u64 (&x)[NP][8], u64 *b0, u64 *b1, const u64 *tw_inv, int t, int bar_id)
+__device__ __forceinline__ void c1_fwd(const u64 *src, u64 *dst, int t)
 {
-    {
-        const int k2b = t >> 5, k1 = t & 31;
+    const int j2a = t >> 5, k1 = t & 31;
+#pragma unroll 1
+    for (int q = 0; q < NP; q++) {
+        const u64 *b = src + q * POLY_WORDS;
+        u64 y[8];
 #pragma unroll
-        for (int q = 0; q < NP; q++) {
-            dit8_inv(x[q]);
-            u64 *b = b0 + q * POLY_WORDS;
+        for (int j2b = 0; j2b < 8; j2b++) y[j2b] = b[k1 * 65 + j2a + 8 * j2b];
+        dif8(y);
+        tw_c1_rt<1>(y, j2a);
+        u64 *o = dst + q * POLY_WORDS;
 #pragma unroll
-            for (int j2a = 0; j2a < 8; j2a++) b[(j2a * 8 + k2b) * 32 + k1] = x[q][j2a];
-        }
+        for (int p = 0; p < 8; p++) o[(j2a * 8 + brv3(p)) * 32 + k1] = y[p];
     }
-    group_sync(bar_id);
-    {
-        const int j2a = t >> 5, k1 = t & 31;
+}
+// C2 of one polynomial: src (C1 layout) -> y, evaluation layout
+__device__ __forceinline__ void c2_fwd(const u64 *src, u64 *y, int t)
+{
+    const int k2b = t >> 5, k1 = t & 31;
 #pragma unroll
-        for (int q = 0; q < NP; q++) {
-            const u64 *b = b0 + q * POLY_WORDS;
+    for (int j2a = 0; j2a < 8; j2a++) y[j2a] = src[(j2a * 8 + k2b) * 32 + k1];
+    dif8(y);
+}
+// C2^-1 of one polynomial held in registers (evaluation layout) -> dst
+__device__ __forceinline__ void c2_inv(u64 *y, u64 *dst, int t)
+{
+    const int k2b = t >> 5, k1 = t & 31;
+    dit8_inv(y);
 #pragma unroll
-            for (int p = 0; p < 8; p++) x[q][p] = b[(j2a * 8 + brv3(p)) * 32 + k1];
-        }
+    for (int j2a = 0; j2a < 8; j2a++) dst[(j2a * 8 + k2b) * 32 + k1] = y[j2a];
+}
+// C1^-1 of NP polynomials: src (C1 layout) -> dst (padded k1 layout)
+template <int NP>
+__device__ __forceinline__ void c1_inv(const u64 *src, u64 *dst, int t)
+{
+    const int j2a = t >> 5, k1 = t & 31;
+#pragma unroll 1
+    for (int q = 0; q < NP; q++) {
+        const u64 *b = src + q * POLY_WORDS;
+        u64 y[8];
 #pragma unroll
-        for (int q = 0; q < NP; q++) {
-            tw_c1_rt<-1>(x[q], j2a);
-            dit8_inv(x[q]);
-            u64 *b = b1 + q * POLY_WORDS;
+        for (int p = 0; p < 8; p++) y[p] = b[(j2a * 8 + brv3(p)) * 32 + k1];
+        tw_c1_rt<-1>(y, j2a);
+        dit8_inv(y);
+        u64 *o = dst + q * POLY_WORDS;
 #pragma unroll
-            for (int j2b = 0; j2b < 8; j2b++) b[k1 * 65 + j2a + 8 * j2b] = x[q][j2b];
-        }
+        for (int j2b = 0; j2b < 8; j2b++) o[k1 * 65 + j2a + 8 * j2b] = y[j2b];
     }
-    group_sync(bar_id);
-    {
-        const int kp = t >> 6, j2 = t & 63;
+}
+// B^-1 + A2^-1 of NP polynomials: src (padded k1 layout) -> dst (A1 layout)
+template <int NP>
+__device__ __forceinline__ void a2_inv(const u64 *src, u64 *dst, const u64 *tw_inv, int t)
+{
+    const int kp = t >> 6, j2 = t & 63;
+#pragma unroll 1
+    for (int q = 0; q < NP; q++) {
+        const u64 *b = src + q * POLY_WORDS;
+        u64 y[8];
 #pragma unroll
-        for (int q = 0; q < NP; q++) {
-            const u64 *b = b1 + q * POLY_WORDS;
+        for (int s = 0; s < 8; s++)
+            y[s] = gl::mul(b[(kp + 4 * (s >> 2) + 8 * brv2(s & 3)) * 65 + j2], tw_inv[s * TPG + t]);
+        dit4_inv(y);
+        dit4_inv(y + 4);
+        u64 *o = dst + q * POLY_WORDS;
 #pragma unroll
-            for (int s = 0; s < 8; s++)
-                x[q][s] = gl::mul(b[(kp + 4 * (s >> 2) + 8 * brv2(s & 3)) * 65 + j2], tw_inv[s * TPG + t]);
-        }
+        for (int c = 0; c < 2; c++)
 #pragma unroll
-        for (int q = 0; q < NP; q++) {
-            dit4_inv(x[q]);
-            dit4_inv(x[q] + 4);
-            u64 *b = b0 + q * POLY_WORDS;
-#pragma unroll
-            for (int c = 0; c < 2; c++)
-#pragma unroll
-                for (int j1a = 0; j1a < 4; j1a++) b[(j1a * 8 + kp + 4 * c) * 64 + j2] = x[q][c * 4 + j1a];
-        }
+            for (int j1a = 0; j1a < 4; j1a++) o[(j1a * 8 + kp + 4 * c) * 64 + j2] = y[c * 4 + j1a];
     }
-    group_sync(bar_id);
-    {
-        const int j1a = t >> 6, j2 = t & 63;
+}
+// A1^-1 of one polynomial: src (A1 layout) -> y, coefficient layout (times N)
+__device__ __forceinline__ void a1_inv(const u64 *src, u64 *y, int t)
+{
+    const int j1a = t >> 6, j2 = t & 63;
 #pragma unroll
-        for (int q = 0; q < NP; q++) {
-            const u64 *b = b0 + q * POLY_WORDS;
-#pragma unroll
-            for (int p = 0; p < 8; p++) x[q][p] = b[(j1a * 8 + brv3(p)) * 64 + j2];
-            tw_a1_rt<-1>(x[q], j1a);
-            gs8_neg_inv(x[q]);
-        }
-    }
+    for (int p = 0; p < 8; p++) y[p] = src[(j1a * 8 + brv3(p)) * 64 + j2];
+    tw_a1_rt<-1>(y, j1a);
+    gs8_neg_inv(y);
 }
 
 // Coefficient index held by thread t in slot e of the coefficient layout.
