@@ -141,7 +141,30 @@ __device__ __forceinline__ void tw_a1(u64 *y)
     y[6] = gl::shl<SIGN * 3 * J1A * (2 * brv3(6) + 1)>(y[6]);
     y[7] = gl::shl<SIGN * 3 * J1A * (2 * brv3(7) + 1)>(y[7]);
 }
-// Runtime forms: one copy of the shift code for every warp-uniform j1a / j2a
+// 2^e mod p for e in [0, 192), built at compile time: the runtime pass
+// twiddles below are one multiply by a constant-cache word (the exponent is
+// warp-uniform, so every lane reads the same word).  A branch-free multiply
+// is shorter code than a shift with its range cases, and half of its work
+// runs on the multiply pipe instead of the saturated integer ALU.
+struct Pow2Table {
+    u64 v[192];
+};
+__host__ __device__ constexpr Pow2Table make_pow2_table()
+{
+    Pow2Table t{};
+    u64 x = 1;
+    for (int e = 0; e < 192; e++) {
+        t.v[e] = x;
+        const bool top = (x >> 63) != 0;
+        u64 y = x << 1;
+        if (top || y >= gl::P) y -= gl::P;  // 2x < 2p: one subtraction (mod 2^64)
+        x = y;
+    }
+    return t;
+}
+static __constant__ Pow2Table c_pow2 = make_pow2_table();
+
+// Runtime forms: one copy of the twiddle code for every warp-uniform j1a / j2a
 // (the templated forms above, one per value, overflow the instruction cache).
 template <int SIGN>
 __device__ __forceinline__ void tw_a1_rt(u64 *y, int j1a)
@@ -150,7 +173,7 @@ __device__ __forceinline__ void tw_a1_rt(u64 *y, int j1a)
 #pragma unroll
     for (int p = 0; p < 8; p++) {
         const u32 e = 3u * j1a * (2 * brv3(p) + 1);  // < 192
-        y[p] = gl::shl_rt(y[p], SIGN > 0 ? e : (192u - e) % 192u);
+        y[p] = gl::mul(y[p], c_pow2.v[SIGN > 0 ? e : (192u - e) % 192u]);
     }
 }
 template <int J2A, int SIGN>
@@ -172,7 +195,7 @@ __device__ __forceinline__ void tw_c1_rt(u64 *y, int j2a)
 #pragma unroll
     for (int p = 1; p < 8; p++) {  // p = 0 has k2b = 0: twiddle 1
         const u32 e = 3u * j2a * brv3(p);  // < 192
-        y[p] = gl::shl_rt(y[p], SIGN > 0 ? e : (192u - e) % 192u);
+        y[p] = gl::mul(y[p], c_pow2.v[SIGN > 0 ? e : (192u - e) % 192u]);
     }
 }
 
