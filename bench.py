@@ -101,22 +101,30 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def read_traffic(B):
-    """DRAM bytes of one blind-rotation launch over B ciphertexts, from the
-    committed ncu summary (profiles/br_kernel_ncu.md): the BSK read once per
-    launch (fixed) plus the per-ciphertext input/output bytes, both measured on
-    the captured 296-ciphertext launch."""
-    path = os.path.join(ROOT, "profiles", "br_kernel_ncu.md")
-    if not os.path.exists(path):
-        return None
+def _profile_values(name, keys):
+    path = os.path.join(ROOT, "profiles", name)
     vals = {}
-    for line in open(path):
-        k, _, v = line.partition(":")
-        if k.strip() in ("dram_bytes_fixed_per_launch", "dram_bytes_per_bootstrap"):
-            vals[k.strip()] = float(v)
-    if len(vals) < 2:
-        return None
-    return vals["dram_bytes_fixed_per_launch"] + vals["dram_bytes_per_bootstrap"] * B
+    if os.path.exists(path):
+        for line in open(path):
+            k, _, v = line.partition(":")
+            if k.strip() in keys:
+                vals[k.strip()] = float(v)
+    return vals
+
+
+def read_traffic(B):
+    """DRAM bytes (read + write) of one blind-rotation launch over B
+    ciphertexts: the ncu figure of the bench's own full-size launch
+    (profiles/br_kernel_traffic.md) when it was taken at this B, else the
+    296-ciphertext capture (profiles/br_kernel_ncu.md) scaled as the BSK read
+    once per launch plus the per-ciphertext bytes.  Returns (bytes, how)."""
+    full = _profile_values("br_kernel_traffic.md", ("ciphertexts_per_launch", "dram_bytes_per_launch"))
+    if full.get("ciphertexts_per_launch") == B and "dram_bytes_per_launch" in full:
+        return full["dram_bytes_per_launch"], "ncu, this launch size"
+    small = _profile_values("br_kernel_ncu.md", ("dram_bytes_fixed_per_launch", "dram_bytes_per_bootstrap"))
+    if len(small) < 2:
+        return None, None
+    return small["dram_bytes_fixed_per_launch"] + small["dram_bytes_per_bootstrap"] * B, "ncu, scaled from 296"
 
 
 def reference_arm(args):
@@ -427,7 +435,7 @@ def main():
     br_s = statistics.median(br_ms) * 1e-3
     imad_peak, glmul_peak = L.measure_int_peak(local)
     achieved_imad = B * MODMUL_PER_BOOTSTRAP * IMAD_PER_MODMUL / br_s
-    traffic = read_traffic(B)
+    traffic, traffic_how = read_traffic(B)
 
     # ---- plain path: one ciphertext per launch
     plain_ms = []
@@ -548,7 +556,7 @@ def main():
                          "peak": imad_peak / 1e12, "unit": "TIMAD/s", "frac": achieved_imad / imad_peak,
                          "peak_source": "measured live (luthe_measure_int_peak, 32-bit IMAD probe)",
                          "work": f"{MODMUL_PER_BOOTSTRAP} modmul x {IMAD_PER_MODMUL} IMAD per bootstrap",
-                         "traffic": traffic, "traffic_unit": "bytes per launch (ncu, scaled)",
+                         "traffic": traffic, "traffic_unit": f"DRAM bytes per launch ({traffic_how})",
                          "modmul_frac": B * MODMUL_PER_BOOTSTRAP / br_s / glmul_peak,
                          "glmul_peak_per_s": glmul_peak, "br_ms": br_s * 1e3},
             "cpu_baseline": cpu,
