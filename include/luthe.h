@@ -186,7 +186,11 @@ int luthe_server_counters(luthe_server *srv, uint64_t *rounds, uint64_t *pbs, ui
 int luthe_set_br_config(luthe_ctx *ctx, int cts_per_cta, int ctas_per_sm);
 int luthe_autotune(luthe_ctx *ctx, size_t sample, char *json, size_t json_cap);
 
-/* Device-side error flag of the last blind rotation (bounded waits). */
+/* Device-side error flags raised by blind rotations since the last check
+ * (sticky, cleared by this call; the stream must have been synchronised):
+ * LUTHE_E_TIMEOUT when a bounded wait for a BSK slab ran out, LUTHE_E_PARAM
+ * when a device-resident LUT id was >= the uploaded LUT count (that
+ * ciphertext was rotated against LUT 0; its output is not meaningful). */
 int luthe_check_device_error(luthe_ctx *ctx);
 
 /* Integer-pipe peaks of `device` measured by probe kernels: 32-bit IMAD per

@@ -407,7 +407,10 @@ extern "C" int luthe_check_device_error(luthe_ctx *c)
     CUDA_TRY(cudaMemcpy(&e, c->d_err, 4, cudaMemcpyDeviceToHost));
     if (e) {
         cudaMemset(c->d_err, 0, 4);
-        return fail(LUTHE_E_TIMEOUT, "blind rotation: bounded wait for a BSK slab ran out");
+        if (e & DEVERR_TIMEOUT)
+            return fail(LUTHE_E_TIMEOUT, "blind rotation: bounded wait for a BSK slab ran out%s",
+                        (e & DEVERR_LUT_ID) ? " (and a LUT id was out of range)" : "");
+        return fail(LUTHE_E_PARAM, "blind rotation: a LUT id was >= the uploaded LUT count (%u)", c->nlut);
     }
     return LUTHE_OK;
 }

@@ -451,7 +451,10 @@ __global__ void __launch_bounds__(G * 256, 1)
         const u32 ct = active ? cidx : B - 1;
         const u32 *my_lwe = lwe2N + (size_t)ct * (n + 1);  // read in place; every thread of the group loads the same word
         u32 lid = lut_id[ct];
-        if (lid >= nlut) lid = 0;  // host validates ids; keep the read in bounds regardless
+        if (lid >= nlut) {  // device-resident ids cannot be checked by the host: flag it, stay in bounds
+            if (t == 0) atomicOr(err, DEVERR_LUT_ID);
+            lid = 0;
+        }
         const u64 *lut = luts + (size_t)lid * 2 * N;
         // ACC: registers (coefficient layout, 16 coefficients per thread), copied
         // to the thread's own slots of bp at the start of every step
@@ -583,7 +586,7 @@ __global__ void __launch_bounds__(G * 256, 1)
         if (!ok) {
             if (t == 0) {
                 atomicExch(failed, 1u);
-                atomicExch(err, 1u);
+                atomicOr(err, DEVERR_TIMEOUT);
             }
         } else if (active) {
             const size_t row0 = dst_idx ? dst_idx[cidx] : (size_t)cidx * mlk;

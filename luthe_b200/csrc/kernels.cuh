@@ -48,6 +48,9 @@ cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n);
 enum LweOp : int { LWE_ADD = 0, LWE_SUB = 1, LWE_MAC = 2, LWE_ADDS = 3, LWE_SUBS = 4, LWE_SSUB = 5, LWE_MULS = 6 };
 // one linear DOp or register copy (op = LWE_COPY) on slots of a BLWE pool
 constexpr int LWE_COPY = 7;
+// device error flag bits (luthe_check_device_error)
+constexpr uint32_t DEVERR_TIMEOUT = 1u;  // a bounded wait for a BSK slab ran out
+constexpr uint32_t DEVERR_LUT_ID = 2u;   // a LUT id >= the uploaded LUT count
 struct AluOp {
     uint32_t op, dst, a, b;
     uint64_t imm;

@@ -167,3 +167,22 @@ def test_errors_are_reported(engine, params):
         engine.set_br_config(3, 1)
     with pytest.raises(L.LutheError):
         engine.ks_pbs_host(np.zeros((1, N + 1), np.uint64), np.array([99], np.uint32))
+
+
+def test_out_of_range_device_lut_id_is_flagged(engine, params, keys, oracle_bsk):
+    # ids on the device cannot be checked by the host: the kernel flags them
+    rng = np.random.default_rng(77)
+    luts = np.stack([L.lut_build(params, rng.integers(0, 16, 16).astype(np.uint32)) for _ in range(2)])
+    engine.upload_luts(luts)
+    ct = L.encrypt(params, keys["glwe_key"], np.array([3, 5, 7], np.uint32), 9)
+    ids = np.array([1, 9, 0], np.uint32)                  # 9 >= 2 uploaded LUTs
+    d_out = to_dev(np.zeros((3, N + 1), np.uint64))
+    engine.ks_pbs(to_dev(ct), to_dev(ids), d_out, 3)
+    with pytest.raises(L.LutheError) as ei:
+        engine.check_device_error()
+    assert ei.value.code == L.E_PARAM
+    engine.check_device_error()                           # the flag was cleared
+    got = from_dev(d_out, np.uint64)
+    ok = np.array([0, 2])                                 # the valid ids are unaffected
+    want = oracle_bsk.ks_pbs(keys["ksk"], ct[ok], luts, ids[ok])
+    assert np.array_equal(got[ok], want)
