@@ -647,11 +647,13 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
 {
     if (B == 0) return cudaSuccess;
     if (mlk != 1 && mlk != 2 && mlk != 4 && mlk != 8) return cudaErrorInvalidValue;
-    const int G = cfg.cts_per_cta;
+    // A batch that fits one ciphertext per SM runs one per CTA: with G = 2 the
+    // second group of each CTA would only duplicate work on the same SM.
+    const int G = (cfg.cts_per_cta > 1 && B <= (size_t)nsm) ? 1 : cfg.cts_per_cta;
     size_t groups = (B + G - 1) / G;
     size_t grid = (size_t)nsm * cfg.ctas_per_sm;
     if (grid > groups) grid = groups;
-    size_t smem = br_smem_bytes(cfg, n);
+    size_t smem = br_smem_bytes(BrConfig{G, cfg.ctas_per_sm}, n);
     u32 Bu = (u32)B;
     void *args[] = {(void *)&d_lwe2N, (void *)&d_luts, (void *)&d_lut_id, (void *)&nlut, (void *)&d_bsk,
                     (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err,

@@ -104,7 +104,9 @@ def _msgs_luts(params, rng, count, nlut):
     return msgs, tables, luts
 
 
-@pytest.mark.parametrize("count", [1, 5])
+# 1 and 5 run one ciphertext per CTA (a batch no larger than the SM count);
+# 301 (> 2 x 148) runs two per CTA with a partial second wave
+@pytest.mark.parametrize("count", [1, 5, 301])
 def test_ks_pbs_bit_exact_and_decrypts(engine, params, keys, oracle_bsk, count):
     rng = np.random.default_rng(60 + count)
     msgs, tables, luts = _msgs_luts(params, rng, count, 3)
