@@ -640,20 +640,15 @@ cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n)
     }
 }
 
-cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_lwe2N, const uint64_t *d_luts,
-                                const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
-                                uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s,
-                                const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw)
+static cudaError_t launch_br_once(int G, int ctas_per_sm, int nsm, const uint32_t *d_lwe2N, const uint64_t *d_luts,
+                                  const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk,
+                                  const uint64_t *d_tw, uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err,
+                                  cudaStream_t s, const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw)
 {
-    if (B == 0) return cudaSuccess;
-    if (mlk != 1 && mlk != 2 && mlk != 4 && mlk != 8) return cudaErrorInvalidValue;
-    // A batch that fits one ciphertext per SM runs one per CTA: with G = 2 the
-    // second group of each CTA would only duplicate work on the same SM.
-    const int G = (cfg.cts_per_cta > 1 && B <= (size_t)nsm) ? 1 : cfg.cts_per_cta;
     size_t groups = (B + G - 1) / G;
-    size_t grid = (size_t)nsm * cfg.ctas_per_sm;
+    size_t grid = (size_t)nsm * ctas_per_sm;
     if (grid > groups) grid = groups;
-    size_t smem = br_smem_bytes(BrConfig{G, cfg.ctas_per_sm}, n);
+    size_t smem = br_smem_bytes(BrConfig{G, ctas_per_sm}, n);
     u32 Bu = (u32)B;
     void *args[] = {(void *)&d_lwe2N, (void *)&d_luts, (void *)&d_lut_id, (void *)&nlut, (void *)&d_bsk,
                     (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err,
@@ -662,8 +657,39 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
     if (G == 1) k = pbs_bw == 22 ? (const void *)br_kernel<1, 22> : (const void *)br_kernel<1, 23>;
     else if (G == 2) k = pbs_bw == 22 ? (const void *)br_kernel<2, 22> : (const void *)br_kernel<2, 23>;
     else return cudaErrorInvalidValue;
-    if (!pbs_supported(pbs_bw)) return cudaErrorInvalidValue;
     return cudaLaunchKernel(k, dim3((unsigned)grid), dim3(256 * G), args, smem, s);
+}
+
+cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_lwe2N, const uint64_t *d_luts,
+                                const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
+                                uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s,
+                                const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw)
+{
+    if (B == 0) return cudaSuccess;
+    if (mlk != 1 && mlk != 2 && mlk != 4 && mlk != 8) return cudaErrorInvalidValue;
+    if (!pbs_supported(pbs_bw)) return cudaErrorInvalidValue;
+    const int G = cfg.cts_per_cta, cps = cfg.ctas_per_sm;
+    const size_t wave = (size_t)nsm * cps * G;
+    // A batch that fits one ciphertext per SM runs one per CTA: with G = 2 the
+    // second group of each CTA would only duplicate work on the same SM.
+    if (G > 1 && B <= (size_t)nsm)
+        return launch_br_once(1, 1, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n, d_err, s,
+                              d_dst_idx, mlk, pbs_bw);
+    // A partial last wave of at most one ciphertext per SM runs as its own
+    // one-per-CTA launch after the full waves: it then takes the time of one
+    // ciphertext-per-SM wave instead of a full G-per-CTA wave.
+    const size_t tail = B % wave;
+    if (G > 1 && B > wave && tail > 0 && tail <= (size_t)nsm) {
+        const size_t full = B - tail;
+        cudaError_t e = launch_br_once(G, cps, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, full, n,
+                                       d_err, s, d_dst_idx, mlk, pbs_bw);
+        if (e != cudaSuccess) return e;
+        uint64_t *out_tail = d_dst_idx ? d_out : d_out + full * mlk * (size_t)(N + 1);
+        return launch_br_once(1, 1, nsm, d_lwe2N + full * (size_t)(n + 1), d_luts, d_lut_id + full, nlut, d_bsk, d_tw,
+                              out_tail, tail, n, d_err, s, d_dst_idx ? d_dst_idx + full : nullptr, mlk, pbs_bw);
+    }
+    return launch_br_once(G, cps, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n, d_err, s,
+                          d_dst_idx, mlk, pbs_bw);
 }
 
 // ---------------------------------------------------------- linear DOps
