@@ -614,6 +614,152 @@ __global__ void __launch_bounds__(G * 256, 1)
     }
 }
 
+// Latency form for batches of at most one ciphertext per SM: one ciphertext
+// per CTA, its two GLWE polynomials split over the two 256-thread groups.
+// Group g owns polynomial g of the accumulator and runs the feed, the forward
+// transform of digit polynomial g, the product for output column g and the
+// inverse transform of column g; the groups meet only around the BSK
+// multiply, which needs both forward transforms (block barriers).  Each step
+// is half the work per group of the one-ciphertext-per-group form, so a
+// lone ciphertext finishes in about half the time.
+template <int BW>
+__global__ void __launch_bounds__(512, 1)
+    br_kernel_split(const u32 *__restrict__ lwe2N, const u64 *__restrict__ luts, const u32 *__restrict__ lut_id,
+                    u32 nlut, const u64 *__restrict__ bsk, const u64 *__restrict__ tw, u64 *__restrict__ out, u32 B,
+                    u32 n, u32 *__restrict__ err, const u32 *__restrict__ dst_idx, u32 mlk)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    u64 *slab = reinterpret_cast<u64 *>(smem_raw);
+    u64 *tws = slab + SLAB_WORDS;
+    u64 *bufs = tws + 4096;  // [group][2 buffers][POLY_WORDS]
+    u64 *mbar = bufs + 4 * POLY_WORDS;
+    const int g = threadIdx.x >> 8, t = threadIdx.x & 255, bar = 1 + g;
+    u64 *bp = bufs + g * 2 * POLY_WORDS, *bq = bp + POLY_WORDS;  // this group's polynomial
+    const u64 *bp0 = bufs, *bp1 = bufs + 2 * POLY_WORDS;          // both groups' bp (MAC operands, extract)
+
+    for (int i = threadIdx.x; i < 4096; i += 512) tws[i] = tw[i];
+    if (threadIdx.x == 0) {
+        mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    u32 phase = 0;
+    for (u32 ct = blockIdx.x; ct < B; ct += gridDim.x) {
+        const u32 *my_lwe = lwe2N + (size_t)ct * (n + 1);
+        u32 lid = lut_id[ct];
+        if (lid >= nlut) {
+            if (threadIdx.x == 0) atomicOr(err, DEVERR_LUT_ID);
+            lid = 0;
+        }
+        const u64 *lut = luts + ((size_t)lid * 2 + g) * N;  // polynomial g of the LUT
+        u64 acc[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int j = ntt::coef_index(t, e);
+            acc[e] = lut[j];
+            bp[j] = acc[e];
+        }
+        if (threadIdx.x == 0) issue_slab(slab, bsk, mbar);
+        __syncthreads();
+
+        // Buffers of group g as in br_kernel (bp: ACC own slots, A2, C2 own
+        // slots, C1^-1; bq: A1, C1, C2^-1, A2^-1); the other group reads this
+        // group's bp own slots only between the two block barriers of the MAC.
+        bool ok = true;
+        u32 a_next = my_lwe[0];
+        for (u32 i = 0; i < n; i++) {
+            const u32 a = a_next;
+            a_next = my_lwe[i + 1];
+            ntt::group_sync(bar);
+            {
+                u64 y[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const u32 j = ntt::coef_index(t, e);
+                    const u32 src = (j + TWO_N - a) & (TWO_N - 1);
+                    u64 v = bp[src & (N - 1)];
+                    if (src >= (u32)N) v = 0ull - v;
+                    y[e] = gl::decomp_to_p<BW>(v - bp[j]);
+                }
+                ntt::a1_fwd(y, bq, t);
+            }
+            ntt::group_sync(bar);
+            ntt::a2_fwd<1>(bq, bp, tws, t);
+            ntt::group_sync(bar);
+            ntt::c1_fwd<1>(bp, bq, t);
+            ntt::group_sync(bar);
+            {
+                u64 y[8];
+                ntt::c2_fwd(bq, y, t);
+#pragma unroll
+                for (int p = 0; p < 8; p++) bp[p * TPG + t] = y[p];  // own slots
+            }
+            ok = mbar_wait(mbar, phase);
+            phase ^= 1;
+            if (__syncthreads_or(!ok)) {  // both transforms written; uniform over the block
+                ok = false;
+                break;
+            }
+            u64 r[8];
+#pragma unroll
+            for (int p = 0; p < 8; p++) {
+                const u64 *sb = slab + p * 4 * TPG + t;  // [row][col]: column g of rows 0 and 1
+                r[p] = gl::mul_add2(bp0[p * TPG + t], sb[g * TPG], bp1[p * TPG + t], sb[(2 + g) * TPG]);
+            }
+            __syncthreads();  // every read of the slab and of the other group's bp is done
+            if (threadIdx.x == 0 && i + 1 < n) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                issue_slab(slab, bsk + (size_t)(i + 1) * SLAB_WORDS, mbar);
+            }
+            ntt::c2_inv(r, bq, t);
+            ntt::group_sync(bar);
+            ntt::c1_inv<1>(bq, bp, t);
+            ntt::group_sync(bar);
+            ntt::a2_inv<1>(bp, bq, tws + 2048, t);
+            ntt::group_sync(bar);
+            {
+                u64 y[8];
+                ntt::a1_inv(bq, y, t);
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const int j = ntt::coef_index(t, e);
+                    acc[e] += gl::modsw_p_to_q(gl::canon(y[e]));
+                    bp[j] = acc[e];
+                }
+            }
+        }
+        __syncthreads();  // both accumulator polynomials complete
+        if (!ok) {        // the block agreed on the timeout above
+            if (threadIdx.x == 0) atomicOr(err, DEVERR_TIMEOUT);
+            return;
+        }
+        // sample extract (as in br_kernel): mask from polynomial 0, body from 1
+        const size_t row0 = dst_idx ? dst_idx[ct] : (size_t)ct * mlk;
+        const u32 body = my_lwe[n];
+        for (u32 m = 0; m < mlk; m++) {
+            const u32 b = (body + m * (N / mlk)) & (TWO_N - 1);
+            u64 *o = out + (row0 + m) * (N + 1);
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const u32 oi = threadIdx.x + 512 * r;
+                const u32 j = oi == 0 ? 0 : N - oi;
+                const u32 src = (j + b) & (TWO_N - 1);
+                u64 v = bp0[src & (N - 1)];
+                if (src >= (u32)N) v = 0ull - v;
+                o[oi] = oi == 0 ? v : 0ull - v;
+            }
+            if (threadIdx.x == 0) {
+                u64 v = bp1[b & (N - 1)];
+                o[N] = b >= (u32)N ? 0ull - v : v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+static size_t br_split_smem_bytes() { return (size_t)(SLAB_WORDS + 4096 + 4 * POLY_WORDS + 1) * 8; }
+
 size_t br_smem_bytes(const BrConfig &cfg, uint32_t n)
 {
     const int G = cfg.cts_per_cta;
@@ -632,7 +778,12 @@ bool pbs_supported(uint32_t bw) { return bw == 23 || bw == 22; }
 cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n)
 {
     size_t smem = br_smem_bytes(cfg, n);
-    cudaError_t e;
+    cudaError_t e = cudaFuncSetAttribute(br_kernel_split<23>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)br_split_smem_bytes());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(br_kernel_split<22>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)br_split_smem_bytes());
+    if (e != cudaSuccess) return e;
     switch (cfg.cts_per_cta) {
     case 1: e = br_attr<1, 23>(smem); return e != cudaSuccess ? e : br_attr<1, 22>(smem);
     case 2: e = br_attr<2, 23>(smem); return e != cudaSuccess ? e : br_attr<2, 22>(smem);
@@ -645,6 +796,15 @@ static cudaError_t launch_br_once(int G, int ctas_per_sm, int nsm, const uint32_
                                   const uint64_t *d_tw, uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err,
                                   cudaStream_t s, const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw)
 {
+    if (G == 0) {  // latency form: one ciphertext per CTA, polynomials split over the groups
+        size_t grid = B < (size_t)nsm ? B : (size_t)nsm;
+        u32 Bu = (u32)B;
+        void *args[] = {(void *)&d_lwe2N, (void *)&d_luts, (void *)&d_lut_id, (void *)&nlut, (void *)&d_bsk,
+                        (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err,
+                        (void *)&d_dst_idx, (void *)&mlk};
+        const void *k = pbs_bw == 22 ? (const void *)br_kernel_split<22> : (const void *)br_kernel_split<23>;
+        return cudaLaunchKernel(k, dim3((unsigned)grid), dim3(512), args, br_split_smem_bytes(), s);
+    }
     size_t groups = (B + G - 1) / G;
     size_t grid = (size_t)nsm * ctas_per_sm;
     if (grid > groups) grid = groups;
@@ -670,14 +830,14 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
     if (!pbs_supported(pbs_bw)) return cudaErrorInvalidValue;
     const int G = cfg.cts_per_cta, cps = cfg.ctas_per_sm;
     const size_t wave = (size_t)nsm * cps * G;
-    // A batch that fits one ciphertext per SM runs one per CTA: with G = 2 the
-    // second group of each CTA would only duplicate work on the same SM.
+    // A batch that fits one ciphertext per SM runs in the latency form (one
+    // ciphertext per CTA, its polynomials split over the two groups): with
+    // G = 2 ciphertexts per CTA half the SMs would idle.
     if (G > 1 && B <= (size_t)nsm)
-        return launch_br_once(1, 1, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n, d_err, s,
+        return launch_br_once(0, 1, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n, d_err, s,
                               d_dst_idx, mlk, pbs_bw);
     // A partial last wave of at most one ciphertext per SM runs as its own
-    // one-per-CTA launch after the full waves: it then takes the time of one
-    // ciphertext-per-SM wave instead of a full G-per-CTA wave.
+    // latency-form launch after the full waves instead of a full G-per-CTA wave.
     const size_t tail = B % wave;
     if (G > 1 && B > wave && tail > 0 && tail <= (size_t)nsm) {
         const size_t full = B - tail;
@@ -685,7 +845,7 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
                                        d_err, s, d_dst_idx, mlk, pbs_bw);
         if (e != cudaSuccess) return e;
         uint64_t *out_tail = d_dst_idx ? d_out : d_out + full * mlk * (size_t)(N + 1);
-        return launch_br_once(1, 1, nsm, d_lwe2N + full * (size_t)(n + 1), d_luts, d_lut_id + full, nlut, d_bsk, d_tw,
+        return launch_br_once(0, 1, nsm, d_lwe2N + full * (size_t)(n + 1), d_luts, d_lut_id + full, nlut, d_bsk, d_tw,
                               out_tail, tail, n, d_err, s, d_dst_idx ? d_dst_idx + full : nullptr, mlk, pbs_bw);
     }
     return launch_br_once(G, cps, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n, d_err, s,
