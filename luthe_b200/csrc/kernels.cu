@@ -1,5 +1,7 @@
 // sm_100a kernels of the KS+PBS engine: BSK preparation, standalone NTTs,
 // the LWE key switch, the persistent blind rotation and the linear DOps.
+#include <cooperative_groups.h>
+
 #include "kernels.cuh"
 #include "ntt.cuh"
 
@@ -760,6 +762,177 @@ __global__ void __launch_bounds__(512, 1)
 
 static size_t br_split_smem_bytes() { return (size_t)(SLAB_WORDS + 4096 + 4 * POLY_WORDS + 1) * 8; }
 
+// Half of a step's BSK slab: column col of both rows, hs[(p*2 + row)*TPG + t]
+// = slab[(p*4 + row*2 + col)*TPG + t] -- sixteen 2 KiB bulk copies.
+__device__ __forceinline__ void issue_half_slab(u64 *hs, const u64 *src, u32 col, u64 *mbar)
+{
+    mbar_expect_tx(mbar, (u32)(SLAB_BYTES / 2));
+#pragma unroll
+    for (int p = 0; p < 8; p++)
+#pragma unroll
+        for (int row = 0; row < 2; row++)
+            bulk_g2s(hs + (p * 2 + row) * TPG, src + (p * 4 + row * 2 + col) * TPG, TPG * 8, mbar);
+}
+
+// More than half an SM's shared memory, so that the two CTAs of a pair never
+// share an SM.
+constexpr size_t PAIR_SMEM_BYTES = 120 * 1024;
+
+// Lowest-latency form, for batches of at most one ciphertext per two SMs: a
+// cluster of two CTAs (256 threads each, one per SM) per ciphertext, CTA r
+// owning polynomial r -- the split form above with the two groups on two
+// SMs.  Each CTA streams only its half of the slab (column r); around the
+// BSK multiply each reads the other's forward transform through distributed
+// shared memory, between cluster barriers.  A slab timeout is agreed by the
+// pair through status flags written into both CTAs' shared memory before the
+// first of those barriers, so both leave the step loop at the same point and
+// every cluster barrier is reached by both.
+template <int BW>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
+    br_kernel_pair(const u32 *__restrict__ lwe2N, const u64 *__restrict__ luts, const u32 *__restrict__ lut_id,
+                   u32 nlut, const u64 *__restrict__ bsk, const u64 *__restrict__ tw, u64 *__restrict__ out, u32 B,
+                   u32 n, u32 *__restrict__ err, const u32 *__restrict__ dst_idx, u32 mlk)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const u32 r = cluster.block_rank();
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    u64 *hs = reinterpret_cast<u64 *>(smem_raw);  // half slab, SLAB_WORDS / 2
+    u64 *tws = hs + SLAB_WORDS / 2;
+    u64 *bp = tws + 4096, *bq = bp + POLY_WORDS;
+    u64 *mbar = bq + POLY_WORDS;
+    u32 *flags = reinterpret_cast<u32 *>(mbar + 1);  // step status of rank 0 and rank 1
+    const int t = threadIdx.x;
+    const u64 *peer_bp = cluster.map_shared_rank(bp, r ^ 1u);
+    u32 *peer_flags = cluster.map_shared_rank(flags, r ^ 1u);
+    const u64 *x0src = r == 0 ? bp : peer_bp, *x1src = r == 0 ? peer_bp : bp;
+
+    for (int i = t; i < 4096; i += TPG) tws[i] = tw[i];
+    if (t == 0) {
+        mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    cluster.sync();  // both CTAs' shared memory is set up before any remote access
+
+    u32 phase = 0;
+    bool ok = true;
+    const u32 npairs = gridDim.x / 2;
+    for (u32 ct = blockIdx.x / 2; ct < B && ok; ct += npairs) {
+        const u32 *my_lwe = lwe2N + (size_t)ct * (n + 1);
+        u32 lid = lut_id[ct];
+        if (lid >= nlut) {
+            if (t == 0 && r == 0) atomicOr(err, DEVERR_LUT_ID);
+            lid = 0;
+        }
+        const u64 *lut = luts + ((size_t)lid * 2 + r) * N;
+        u64 acc[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int j = ntt::coef_index(t, e);
+            acc[e] = lut[j];
+            bp[j] = acc[e];
+        }
+        if (t == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the last reads of hs
+            issue_half_slab(hs, bsk, r, mbar);
+        }
+
+        u32 a_next = my_lwe[0];
+        for (u32 i = 0; i < n; i++) {
+            const u32 a = a_next;
+            a_next = my_lwe[i + 1];
+            __syncthreads();
+            {
+                u64 y[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const u32 j = ntt::coef_index(t, e);
+                    const u32 src = (j + TWO_N - a) & (TWO_N - 1);
+                    u64 v = bp[src & (N - 1)];
+                    if (src >= (u32)N) v = 0ull - v;
+                    y[e] = gl::decomp_to_p<BW>(v - bp[j]);
+                }
+                ntt::a1_fwd(y, bq, t);
+            }
+            __syncthreads();
+            ntt::a2_fwd<1>(bq, bp, tws, t);
+            __syncthreads();
+            ntt::c1_fwd<1>(bp, bq, t);
+            __syncthreads();
+            {
+                u64 y[8];
+                ntt::c2_fwd(bq, y, t);
+#pragma unroll
+                for (int p = 0; p < 8; p++) bp[p * TPG + t] = y[p];  // own slots
+            }
+            const bool cta_ok = !__syncthreads_or(!mbar_wait(mbar, phase));
+            phase ^= 1;
+            if (t == 0) {
+                flags[r] = cta_ok;
+                peer_flags[r] = cta_ok;
+            }
+            cluster.sync();  // both transforms and both status flags are visible
+            if (!(flags[0] && flags[1])) {
+                ok = false;  // same decision in both CTAs
+                break;
+            }
+            u64 rr[8];
+#pragma unroll
+            for (int p = 0; p < 8; p++)
+                rr[p] = gl::mul_add2(x0src[p * TPG + t], hs[(p * 2) * TPG + t], x1src[p * TPG + t],
+                                     hs[(p * 2 + 1) * TPG + t]);
+            __syncthreads();  // every read of the half slab is done
+            if (t == 0 && i + 1 < n) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                issue_half_slab(hs, bsk + (size_t)(i + 1) * SLAB_WORDS, r, mbar);
+            }
+            ntt::c2_inv(rr, bq, t);
+            cluster.sync();  // the other CTA has finished reading this CTA's bp
+            ntt::c1_inv<1>(bq, bp, t);
+            __syncthreads();
+            ntt::a2_inv<1>(bp, bq, tws + 2048, t);
+            __syncthreads();
+            {
+                u64 y[8];
+                ntt::a1_inv(bq, y, t);
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const int j = ntt::coef_index(t, e);
+                    acc[e] += gl::modsw_p_to_q(gl::canon(y[e]));
+                    bp[j] = acc[e];
+                }
+            }
+        }
+        __syncthreads();
+        if (!ok) break;
+        // sample extract: rank 0 writes the mask (polynomial 0), rank 1 the body
+        const size_t row0 = dst_idx ? dst_idx[ct] : (size_t)ct * mlk;
+        const u32 body = my_lwe[n];
+        for (u32 m = 0; m < mlk; m++) {
+            const u32 b = (body + m * (N / mlk)) & (TWO_N - 1);
+            u64 *o = out + (row0 + m) * (N + 1);
+            if (r == 0) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const u32 oi = t + TPG * k;
+                    const u32 j = oi == 0 ? 0 : N - oi;
+                    const u32 src = (j + b) & (TWO_N - 1);
+                    u64 v = bp[src & (N - 1)];
+                    if (src >= (u32)N) v = 0ull - v;
+                    o[oi] = oi == 0 ? v : 0ull - v;
+                }
+            } else if (t == 0) {
+                u64 v = bp[b & (N - 1)];
+                o[N] = b >= (u32)N ? 0ull - v : v;
+            }
+        }
+        __syncthreads();
+    }
+    if (!ok && t == 0 && r == 0) atomicOr(err, DEVERR_TIMEOUT);
+    cluster.sync();  // no CTA leaves while the other may still address its shared memory
+}
+
 size_t br_smem_bytes(const BrConfig &cfg, uint32_t n)
 {
     const int G = cfg.cts_per_cta;
@@ -783,6 +956,12 @@ cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n)
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(br_kernel_split<22>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)br_split_smem_bytes());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(br_kernel_pair<23>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)PAIR_SMEM_BYTES);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(br_kernel_pair<22>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)PAIR_SMEM_BYTES);
     if (e != cudaSuccess) return e;
     switch (cfg.cts_per_cta) {
     case 1: e = br_attr<1, 23>(smem); return e != cudaSuccess ? e : br_attr<1, 22>(smem);
@@ -796,6 +975,15 @@ static cudaError_t launch_br_once(int G, int ctas_per_sm, int nsm, const uint32_
                                   const uint64_t *d_tw, uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err,
                                   cudaStream_t s, const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw)
 {
+    if (G == -1) {  // lowest-latency form: a cluster of two CTAs (two SMs) per ciphertext
+        size_t pairs = B < (size_t)(nsm / 2) ? B : (size_t)(nsm / 2);
+        u32 Bu = (u32)B;
+        void *args[] = {(void *)&d_lwe2N, (void *)&d_luts, (void *)&d_lut_id, (void *)&nlut, (void *)&d_bsk,
+                        (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err,
+                        (void *)&d_dst_idx, (void *)&mlk};
+        const void *k = pbs_bw == 22 ? (const void *)br_kernel_pair<22> : (const void *)br_kernel_pair<23>;
+        return cudaLaunchKernel(k, dim3((unsigned)(2 * pairs)), dim3(TPG), args, PAIR_SMEM_BYTES, s);
+    }
     if (G == 0) {  // latency form: one ciphertext per CTA, polynomials split over the groups
         size_t grid = B < (size_t)nsm ? B : (size_t)nsm;
         u32 Bu = (u32)B;
@@ -833,9 +1021,11 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
     // A batch that fits one ciphertext per SM runs in the latency form (one
     // ciphertext per CTA, its polynomials split over the two groups): with
     // G = 2 ciphertexts per CTA half the SMs would idle.
+    // At most one ciphertext per two SMs: the two-SM form, lower latency still.
+    auto small_form = [&](size_t count) { return count <= (size_t)(nsm / 2) ? -1 : 0; };
     if (G > 1 && B <= (size_t)nsm)
-        return launch_br_once(0, 1, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n, d_err, s,
-                              d_dst_idx, mlk, pbs_bw);
+        return launch_br_once(small_form(B), 1, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n,
+                              d_err, s, d_dst_idx, mlk, pbs_bw);
     // A partial last wave of at most one ciphertext per SM runs as its own
     // latency-form launch after the full waves instead of a full G-per-CTA wave.
     const size_t tail = B % wave;
@@ -845,8 +1035,9 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
                                        d_err, s, d_dst_idx, mlk, pbs_bw);
         if (e != cudaSuccess) return e;
         uint64_t *out_tail = d_dst_idx ? d_out : d_out + full * mlk * (size_t)(N + 1);
-        return launch_br_once(0, 1, nsm, d_lwe2N + full * (size_t)(n + 1), d_luts, d_lut_id + full, nlut, d_bsk, d_tw,
-                              out_tail, tail, n, d_err, s, d_dst_idx ? d_dst_idx + full : nullptr, mlk, pbs_bw);
+        return launch_br_once(small_form(tail), 1, nsm, d_lwe2N + full * (size_t)(n + 1), d_luts, d_lut_id + full,
+                              nlut, d_bsk, d_tw, out_tail, tail, n, d_err, s, d_dst_idx ? d_dst_idx + full : nullptr,
+                              mlk, pbs_bw);
     }
     return launch_br_once(G, cps, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n, d_err, s,
                           d_dst_idx, mlk, pbs_bw);

@@ -104,11 +104,12 @@ def _msgs_luts(params, rng, count, nlut):
     return msgs, tables, luts
 
 
-# On 148 SMs with two ciphertexts per CTA: 1 and 5 run one per CTA (a batch no
-# larger than the SM count); 301 = one full wave + a 5-ciphertext tail launched
-# one per CTA; 450 = one full wave + a partial two-per-CTA wave of 154.  The
-# oracle checks the first ciphertexts and the whole last (partial) wave.
-@pytest.mark.parametrize("count", [1, 5, 301, 450])
+# On 148 SMs with two ciphertexts per CTA: 1 and 5 run one ciphertext per two
+# SMs (cluster pairs); 100 one per SM (polynomials split over the CTA's
+# groups); 301 = one full wave + a 5-ciphertext tail in cluster pairs; 450 =
+# one full wave + a partial two-per-CTA wave of 154.  The oracle checks the
+# first ciphertexts and the ciphertexts after the first wave.
+@pytest.mark.parametrize("count", [1, 5, 100, 301, 450])
 def test_ks_pbs_bit_exact_and_decrypts(engine, params, keys, oracle_bsk, count):
     rng = np.random.default_rng(60 + count)
     msgs, tables, luts = _msgs_luts(params, rng, count, 3)
@@ -122,7 +123,7 @@ def test_ks_pbs_bit_exact_and_decrypts(engine, params, keys, oracle_bsk, count):
     got = from_dev(d_out, np.uint64)
     dec = L.decrypt(params, keys["glwe_key"], got)
     assert [int(d) for d in dec] == [int(tables[i][m]) for i, m in zip(ids, msgs)]
-    check = np.arange(count) if count <= 8 else np.r_[0:4, 296:count]
+    check = np.arange(count) if count <= 8 else np.r_[0:4, 296:count] if count > 296 else np.r_[0:4, count - 4:count]
     want = oracle_bsk.ks_pbs(keys["ksk"], ct[check], luts, ids[check])
     assert np.array_equal(got[check], want)
 
