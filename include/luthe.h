@@ -86,7 +86,11 @@ const char *luthe_last_error(void);
 
 /* Context: binds a CUDA device; `hbm_budget` caps the device bytes the context
  * may hold (0 = 80 GB).  Replaces the HPU bring-up the host backend performs
- * over PCIe (docs/hpu.md:42-54). */
+ * over PCIe (docs/hpu.md:42-54).  Creating a context also sets, for the whole
+ * device, the bound on each blind-rotation wait for a BSK slab: 2^26 polls,
+ * or the value of the environment variable LUTHE_SLAB_WAIT_POLLS (a
+ * diagnostic; 0 makes every wait run out at once, which the tests use to
+ * exercise the timeout path). */
 int luthe_ctx_create(const luthe_params *p, int device, uint64_t hbm_budget, luthe_ctx **out);
 void luthe_ctx_destroy(luthe_ctx *ctx);
 uint64_t luthe_device_bytes(const luthe_ctx *ctx);

@@ -102,6 +102,11 @@ extern "C" int luthe_ctx_create(const luthe_params *p, int device, uint64_t budg
     if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, 4);
     if (e == cudaSuccess) e = br_set_attributes(BrConfig{1, 1}, p->lwe_dim);
     if (e == cudaSuccess) e = br_set_attributes(BrConfig{2, 1}, p->lwe_dim);
+    if (e == cudaSuccess) {
+        // diagnostics: LUTHE_SLAB_WAIT_POLLS bounds each BSK-slab wait (0: run out at once)
+        const char *polls = getenv("LUTHE_SLAB_WAIT_POLLS");
+        e = set_slab_wait_polls(polls ? strtoull(polls, nullptr, 10) : (1ull << 26));
+    }
     if (e != cudaSuccess) {
         luthe_ctx_destroy(c);
         return fail(LUTHE_E_CUDA, "context init: %s", cudaGetErrorString(e));

@@ -360,7 +360,16 @@ cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint
 //   ACC_col += modsw_{p->2^64}(R_col)
 // then the sample extract of X^{-b} ACC (sxt_core.sv:8-14).
 
-constexpr unsigned long long MBAR_SPIN_LIMIT = 1ull << 26;
+// Bound on the polls of one BSK-slab wait (set per device by the host, see
+// set_slab_wait_polls) and on the final wait for copies still in flight.
+constexpr unsigned long long SLAB_WAIT_POLLS_DEFAULT = 1ull << 26;
+constexpr unsigned long long DRAIN_POLLS = 1ull << 26;
+__device__ unsigned long long g_slab_wait_polls = SLAB_WAIT_POLLS_DEFAULT;
+
+cudaError_t set_slab_wait_polls(unsigned long long polls)
+{
+    return cudaMemcpyToSymbol(g_slab_wait_polls, &polls, sizeof polls);
+}
 
 __device__ __forceinline__ u32 smem_addr(const void *p) { return (u32)__cvta_generic_to_shared(p); }
 
@@ -381,11 +390,11 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, u32 bytes, 
         "l"(src), "r"(bytes), "r"(smem_addr(mbar))
         : "memory");
 }
-// bounded wait on the given phase parity; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(u64 *mbar, u32 parity)
+// bounded wait on the given phase parity; returns false after `polls` polls
+__device__ __forceinline__ bool mbar_wait(u64 *mbar, u32 parity, unsigned long long polls)
 {
     u32 a = smem_addr(mbar);
-    for (unsigned long long it = 0; it < MBAR_SPIN_LIMIT; it++) {
+    for (unsigned long long it = 0; it < polls; it++) {
         u32 done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -433,6 +442,8 @@ __global__ void __launch_bounds__(G * 256, 1)
     u64 *mbar = bufs + G * 4 * POLY_WORDS;
     u32 *slab_done = reinterpret_cast<u32 *>(mbar + 1);  // groups that finished the current slab
     u32 *failed = slab_done + 1;
+    u32 *last_parity = failed + 1;  // phase parity of the last slab issued
+    const unsigned long long polls = g_slab_wait_polls;
     const int g = threadIdx.x >> 8, t = threadIdx.x & 255, bar = 1 + g;
     // two staging buffers per ciphertext group (fixed roles, see the step below)
     u64 *bp = bufs + g * 4 * POLY_WORDS, *bq = bp + 2 * POLY_WORDS;
@@ -471,6 +482,7 @@ __global__ void __launch_bounds__(G * 256, 1)
             }
         if (threadIdx.x == 0) {
             *slab_done = 0;
+            *last_parity = phase;
             issue_slab(slab, bsk, mbar);
         }
         __syncthreads();
@@ -526,7 +538,7 @@ __global__ void __launch_bounds__(G * 256, 1)
                 for (int p = 0; p < 8; p++) bp[q * POLY_WORDS + p * TPG + t] = y[p];  // own slots
             }
             // BSK multiply-accumulate in the evaluation domain
-            ok = mbar_wait(mbar, phase);
+            ok = mbar_wait(mbar, phase, polls);
             phase ^= 1;
 #pragma unroll
             for (int p = 0; p < 8; p++) {
@@ -547,6 +559,7 @@ __global__ void __launch_bounds__(G * 256, 1)
                     // every group has read slab i: reuse the buffer for slab i+1
                     __threadfence_block();
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    *last_parity = phase;
                     issue_slab(slab, bsk + (size_t)(i + 1) * SLAB_WORDS, mbar);
                 }
             }
@@ -612,7 +625,12 @@ __global__ void __launch_bounds__(G * 256, 1)
             }
         }
         __syncthreads();
-        if (*failed) return;  // read by every thread after the barrier: uniform
+        if (*failed) {  // read by every thread after the barrier: uniform
+            // the last slab issued may still be landing in this block's shared
+            // memory: wait for it (bounded) before the block ends
+            if (threadIdx.x == 0) mbar_wait(mbar, *last_parity, DRAIN_POLLS);
+            return;
+        }
     }
 }
 
@@ -635,6 +653,8 @@ __global__ void __launch_bounds__(512, 1)
     u64 *tws = slab + SLAB_WORDS;
     u64 *bufs = tws + 4096;  // [group][2 buffers][POLY_WORDS]
     u64 *mbar = bufs + 4 * POLY_WORDS;
+    u32 *last_parity = reinterpret_cast<u32 *>(mbar + 1);  // phase parity of the last slab issued
+    const unsigned long long polls = g_slab_wait_polls;
     const int g = threadIdx.x >> 8, t = threadIdx.x & 255, bar = 1 + g;
     u64 *bp = bufs + g * 2 * POLY_WORDS, *bq = bp + POLY_WORDS;  // this group's polynomial
     const u64 *bp0 = bufs, *bp1 = bufs + 2 * POLY_WORDS;          // both groups' bp (MAC operands, extract)
@@ -662,7 +682,10 @@ __global__ void __launch_bounds__(512, 1)
             acc[e] = lut[j];
             bp[j] = acc[e];
         }
-        if (threadIdx.x == 0) issue_slab(slab, bsk, mbar);
+        if (threadIdx.x == 0) {
+            *last_parity = phase;
+            issue_slab(slab, bsk, mbar);
+        }
         __syncthreads();
 
         // Buffers of group g as in br_kernel (bp: ACC own slots, A2, C2 own
@@ -697,7 +720,7 @@ __global__ void __launch_bounds__(512, 1)
 #pragma unroll
                 for (int p = 0; p < 8; p++) bp[p * TPG + t] = y[p];  // own slots
             }
-            ok = mbar_wait(mbar, phase);
+            ok = mbar_wait(mbar, phase, polls);
             phase ^= 1;
             if (__syncthreads_or(!ok)) {  // both transforms written; uniform over the block
                 ok = false;
@@ -712,6 +735,7 @@ __global__ void __launch_bounds__(512, 1)
             __syncthreads();  // every read of the slab and of the other group's bp is done
             if (threadIdx.x == 0 && i + 1 < n) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                *last_parity = phase;
                 issue_slab(slab, bsk + (size_t)(i + 1) * SLAB_WORDS, mbar);
             }
             ntt::c2_inv(r, bq, t);
@@ -733,7 +757,10 @@ __global__ void __launch_bounds__(512, 1)
         }
         __syncthreads();  // both accumulator polynomials complete
         if (!ok) {        // the block agreed on the timeout above
-            if (threadIdx.x == 0) atomicOr(err, DEVERR_TIMEOUT);
+            if (threadIdx.x == 0) {
+                atomicOr(err, DEVERR_TIMEOUT);
+                mbar_wait(mbar, *last_parity, DRAIN_POLLS);  // a slab still landing here
+            }
             return;
         }
         // sample extract (as in br_kernel): mask from polynomial 0, body from 1
@@ -760,7 +787,7 @@ __global__ void __launch_bounds__(512, 1)
     }
 }
 
-static size_t br_split_smem_bytes() { return (size_t)(SLAB_WORDS + 4096 + 4 * POLY_WORDS + 1) * 8; }
+static size_t br_split_smem_bytes() { return (size_t)(SLAB_WORDS + 4096 + 4 * POLY_WORDS + 2) * 8; }
 
 // Half of a step's BSK slab: column col of both rows, hs[(p*2 + row)*TPG + t]
 // = slab[(p*4 + row*2 + col)*TPG + t] -- sixteen 2 KiB bulk copies.
@@ -802,6 +829,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     u64 *bp = tws + 4096, *bq = bp + POLY_WORDS;
     u64 *mbar = bq + POLY_WORDS;
     u32 *flags = reinterpret_cast<u32 *>(mbar + 1);  // step status of rank 0 and rank 1
+    u32 *last_parity = flags + 2;                     // phase parity of the last half slab issued
+    const unsigned long long polls = g_slab_wait_polls;
     const int t = threadIdx.x;
     const u64 *peer_bp = cluster.map_shared_rank(bp, r ^ 1u);
     u32 *peer_flags = cluster.map_shared_rank(flags, r ^ 1u);
@@ -835,6 +864,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
         }
         if (t == 0) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the last reads of hs
+            *last_parity = phase;
             issue_half_slab(hs, bsk, r, mbar);
         }
 
@@ -866,7 +896,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
 #pragma unroll
                 for (int p = 0; p < 8; p++) bp[p * TPG + t] = y[p];  // own slots
             }
-            const bool cta_ok = !__syncthreads_or(!mbar_wait(mbar, phase));
+            const bool cta_ok = !__syncthreads_or(!mbar_wait(mbar, phase, polls));
             phase ^= 1;
             if (t == 0) {
                 flags[r] = cta_ok;
@@ -885,6 +915,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
             __syncthreads();  // every read of the half slab is done
             if (t == 0 && i + 1 < n) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                *last_parity = phase;
                 issue_half_slab(hs, bsk + (size_t)(i + 1) * SLAB_WORDS, r, mbar);
             }
             ntt::c2_inv(rr, bq, t);
@@ -929,7 +960,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
         }
         __syncthreads();
     }
-    if (!ok && t == 0 && r == 0) atomicOr(err, DEVERR_TIMEOUT);
+    if (!ok && t == 0) {
+        if (r == 0) atomicOr(err, DEVERR_TIMEOUT);
+        mbar_wait(mbar, *last_parity, DRAIN_POLLS);  // a half slab still landing here
+    }
     cluster.sync();  // no CTA leaves while the other may still address its shared memory
 }
 
@@ -937,7 +971,7 @@ size_t br_smem_bytes(const BrConfig &cfg, uint32_t n)
 {
     const int G = cfg.cts_per_cta;
     (void)n;
-    return (size_t)(SLAB_WORDS + 4096 + G * 4 * POLY_WORDS + 2) * 8;
+    return (size_t)(SLAB_WORDS + 4096 + G * 4 * POLY_WORDS + 3) * 8;
 }
 
 template <int G, int BW>

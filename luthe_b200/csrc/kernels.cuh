@@ -38,6 +38,9 @@ cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint
                              const uint32_t *d_src_idx = nullptr, uint32_t bl = KS_BL, uint32_t L = KS_L);
 bool ks_supported(uint32_t bl, uint32_t L);
 bool pbs_supported(uint32_t bw);
+// Bound on the polls of each BSK-slab wait of the blind rotation on the
+// current device (default 2^26); 0 makes every wait run out at once.
+cudaError_t set_slab_wait_polls(unsigned long long polls);
 cudaError_t launch_blind_rotate(const BrConfig &cfg, int num_sms, const uint32_t *d_lwe2N, const uint64_t *d_luts,
                                 const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
                                 uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s,
