@@ -532,7 +532,12 @@ def main():
         other["keyswitch_16384"]["cpu"] = cpu_keyswitch(*ks_sample, keys["ksk"], params)
 
     # ---- serving loop (one GPU): Poisson arrivals of radix IOps
-    serve = serving(L, eng, params, keys, args.seed + 99) if world == 1 and not args.no_serving else None
+    # at 300 req/s offered (above the loop's capacity for this mix: the queue
+    # grows) and at 150 req/s (inside it)
+    serve = serve_light = None
+    if world == 1 and not args.no_serving:
+        serve = serving(L, eng, params, keys, args.seed + 99)
+        serve_light = serving(L, eng, params, keys, args.seed + 98, rate=150.0)
 
     # ---- CPU baseline (rank 0, one GPU): the CPU restatement on all host cores
     cpu = None
@@ -580,6 +585,7 @@ def main():
             "clocks": clk,
             "autotune": tune.get("chosen"),
             "serving": serve,
+            "serving_150": serve_light,
             "other_configs": other,
             "param_sets": psets,
         }
