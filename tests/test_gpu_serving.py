@@ -26,25 +26,30 @@ def dec_blocks(params, keys, blwe):
     return [int(x) for x in L.decrypt(params, keys["glwe_key"], blwe)]
 
 
-@pytest.mark.parametrize("mlk", [2, 4])
-def test_many_lut_matches_oracle(engine, params, keys, oracle_bsk, mlk):
-    rng = np.random.default_rng(100 + mlk)
+# 5 and 3 ciphertexts run in the two-SM form; 301 = a full two-per-CTA wave
+# plus a 5-ciphertext tail launch whose outputs start at row 296 * mlk
+@pytest.mark.parametrize("mlk,count", [(2, 5), (4, 5), (8, 3), (2, 301)])
+def test_many_lut_matches_oracle(engine, params, keys, oracle_bsk, mlk, count):
+    rng = np.random.default_rng(100 + mlk + count)
     span = 16 // mlk
     fs = [rng.integers(0, 16, span).astype(np.uint32) for _ in range(mlk)]
     table = np.concatenate(fs)
     luts = L.lut_build(params, table)[None]
-    msgs = rng.integers(0, span, 5).astype(np.uint32)
+    msgs = rng.integers(0, span, count).astype(np.uint32)
     ct = L.encrypt(params, keys["glwe_key"], msgs, 300 + mlk)
     engine.upload_luts(luts)
-    ids = np.zeros(5, np.uint32)
-    d_out = to_dev(np.zeros((5 * mlk, N + 1), np.uint64))
-    engine.ks_pbs_ml(to_dev(ct), to_dev(ids), d_out, 5, mlk)
+    engine.set_br_config(2, 1)
+    ids = np.zeros(count, np.uint32)
+    d_out = to_dev(np.zeros((count * mlk, N + 1), np.uint64))
+    engine.ks_pbs_ml(to_dev(ct), to_dev(ids), d_out, count, mlk)
     engine.check_device_error()
     got = from_dev(d_out, np.uint64)
-    want = oracle_bsk.ks_pbs(keys["ksk"], ct, luts, ids, mlk=mlk)
-    assert np.array_equal(got, want)
     dec = dec_blocks(params, keys, got)
     assert dec == [int(fs[m][x]) for x in msgs for m in range(mlk)]
+    check = np.arange(count) if count <= 8 else np.r_[0:3, 296:count]
+    rows = (check[:, None] * mlk + np.arange(mlk)).ravel()
+    want = oracle_bsk.ks_pbs(keys["ksk"], ct[check], luts, ids[check], mlk=mlk)
+    assert np.array_equal(got[rows], want)
 
 
 def oracle_run(program, src, n_dst, keys, oracle_bsk, luts):
