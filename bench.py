@@ -326,9 +326,11 @@ def br_launches_per_step(B, nsm, g):
 
 def config_dict():
     return {
-        "workload": "batched KS+PBS of uneven batches 1+17+256+1000+4096 = 5370 BLWEs in one launch, "
+        "workload": "batched KS+PBS of uneven batches 1+17+256+1000+4096 = 5370 BLWEs in one call, "
                     "each batch its own random 4-bit LUT; TFHE n=804 k=1 N=2048 PBS 23x1 KS 3x6 mod 2^21, "
                     "NTT mod 2^64-2^32+1",
+        "launch": "one CUDA graph per step (luthe_ks_pbs_graph): key switch + persistent blind rotation "
+                  "(+ a tail launch when the last wave is partial)",
         "batches": BATCHES, "ciphertexts_per_step": sum(BATCHES),
         "l2": "flushed between timed steps (256 MiB device write); BSK 52.7 MB and KSK 44 MB are L2-resident "
               "by design inside a step",
@@ -394,12 +396,17 @@ def main():
     d_out = torch.empty_like(d_in)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream()
+    # the step is replayed from a CUDA graph (luthe_ks_pbs_graph: captured on
+    # the first call, a non-default stream); flush and events go on that stream
+    gstream = torch.cuda.Stream()
 
     def step():
-        eng.ks_pbs(d_in, d_ids, d_out, B, stream)
+        eng.ks_pbs_graph(d_in, d_ids, d_out, B, gstream)
 
+    torch.cuda.synchronize()
     for _ in range(args.warmup):
-        flush.fill_(1)
+        with torch.cuda.stream(gstream):
+            flush.fill_(1)
         step()
     torch.cuda.synchronize()
     eng.check_device_error()
@@ -414,11 +421,12 @@ def main():
     clocks.start()
     evs = []
     for k in range(args.steps):
-        flush.fill_(k)
+        with torch.cuda.stream(gstream):
+            flush.fill_(k)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        e0.record(gstream)
         step()
-        e1.record(stream)
+        e1.record(gstream)
         evs.append((e0, e1))
     torch.cuda.synchronize()
     clk = clocks.stop()
