@@ -639,9 +639,10 @@ __global__ void __launch_bounds__(G * 256, 1)
 // Group g owns polynomial g of the accumulator and runs the feed, the forward
 // transform of digit polynomial g, the product for output column g and the
 // inverse transform of column g; the groups meet only around the BSK
-// multiply, which needs both forward transforms (block barriers).  Each step
-// is half the work per group of the one-ciphertext-per-group form, so a
-// lone ciphertext finishes in about half the time.
+// multiply, which needs both forward transforms (block barriers).  Each group
+// does half of a step's work, but one SM's integer throughput still bounds a
+// lone ciphertext: measured about 10 % faster than one ciphertext per group.
+// The two-SM form below halves the work per SM.
 template <int BW>
 __global__ void __launch_bounds__(512, 1)
     br_kernel_split(const u32 *__restrict__ lwe2N, const u64 *__restrict__ luts, const u32 *__restrict__ lut_id,
@@ -1004,6 +1005,9 @@ cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n)
     }
 }
 
+// One blind-rotation launch.  G: ciphertexts per CTA (1 or 2, br_kernel);
+// 0: one ciphertext per CTA split over its two groups (br_kernel_split);
+// -1: one ciphertext per cluster of two CTAs (br_kernel_pair).
 static cudaError_t launch_br_once(int G, int ctas_per_sm, int nsm, const uint32_t *d_lwe2N, const uint64_t *d_luts,
                                   const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk,
                                   const uint64_t *d_tw, uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err,
