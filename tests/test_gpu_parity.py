@@ -192,3 +192,25 @@ def test_out_of_range_device_lut_id_is_flagged(engine, params, keys, oracle_bsk)
     ok = np.array([0, 2])                                 # the valid ids are unaffected
     want = oracle_bsk.ks_pbs(keys["ksk"], ct[ok], luts, ids[ok])
     assert np.array_equal(got[ok], want)
+
+
+def test_graph_replay_of_wave_and_tail_equals_direct_launches(engine, params, keys):
+    # 301 BLWEs: a two-per-CTA wave plus a tail launch, captured in one graph
+    import torch
+    rng = np.random.default_rng(90)
+    msgs, tables, luts = _msgs_luts(params, rng, 301, 2)
+    ids = rng.integers(0, 2, 301).astype(np.uint32)
+    ct = L.encrypt(params, keys["glwe_key"], msgs, 91)
+    engine.upload_luts(luts)
+    engine.set_br_config(2, 1)
+    d_in, d_ids = to_dev(ct), to_dev(ids)
+    d_direct, d_graph = to_dev(np.zeros_like(ct)), to_dev(np.zeros_like(ct))
+    engine.ks_pbs(d_in, d_ids, d_direct, 301)
+    s = torch.cuda.Stream()
+    for _ in range(2):  # capture, then replay
+        engine.ks_pbs_graph(d_in, d_ids, d_graph, 301, s)
+    s.synchronize()
+    engine.check_device_error()
+    assert np.array_equal(from_dev(d_graph, np.uint64), from_dev(d_direct, np.uint64))
+    dec = L.decrypt(params, keys["glwe_key"], from_dev(d_graph, np.uint64))
+    assert [int(d) for d in dec] == [int(tables[i][m]) for i, m in zip(ids, msgs)]
