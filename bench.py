@@ -453,6 +453,7 @@ def main():
     imad_peak, glmul_peak = L.measure_int_peak(local)
     achieved_imad = B * MODMUL_PER_BOOTSTRAP * IMAD_PER_MODMUL / br_s
     traffic, traffic_how = read_traffic(B)
+    pipes = _profile_values("br_kernel_ncu.md", ("alu_pipe_busy", "fma_pipe_busy", "issue_active"))
 
     # ---- plain path: one ciphertext per launch
     plain_ms = []
@@ -585,7 +586,9 @@ def main():
                          "work": f"{MODMUL_PER_BOOTSTRAP} modmul x {IMAD_PER_MODMUL} IMAD per bootstrap",
                          "traffic": traffic, "traffic_unit": f"DRAM bytes per launch ({traffic_how})",
                          "modmul_frac": B * MODMUL_PER_BOOTSTRAP / br_s / glmul_peak,
-                         "glmul_peak_per_s": glmul_peak, "br_ms": br_s * 1e3},
+                         "glmul_peak_per_s": glmul_peak, "br_ms": br_s * 1e3,
+                         "pipe_utilisation_ncu": dict(pipes, source="profiles/br_kernel_ncu.md (296-BLWE wave)")
+                         if pipes else None},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(ct.nbytes + ids.nbytes),
                     "d2h_bytes_per_step": int(ct.nbytes), "ms_per_step": statistics.mean(e2e_ms)},
