@@ -26,9 +26,10 @@ def dec_blocks(params, keys, blwe):
     return [int(x) for x in L.decrypt(params, keys["glwe_key"], blwe)]
 
 
-# 5 and 3 ciphertexts run in the two-SM form; 301 = a full two-per-CTA wave
-# plus a 5-ciphertext tail launch whose outputs start at row 296 * mlk
-@pytest.mark.parametrize("mlk,count", [(2, 5), (4, 5), (8, 3), (2, 301)])
+# 5 and 3 ciphertexts run in the two-SM form, 100 in the one-per-SM form;
+# 301 = a full two-per-CTA wave plus a 5-ciphertext tail launch whose outputs
+# start at row 296 * mlk
+@pytest.mark.parametrize("mlk,count", [(2, 5), (4, 5), (8, 3), (4, 100), (2, 301)])
 def test_many_lut_matches_oracle(engine, params, keys, oracle_bsk, mlk, count):
     rng = np.random.default_rng(100 + mlk + count)
     span = 16 // mlk
@@ -46,7 +47,7 @@ def test_many_lut_matches_oracle(engine, params, keys, oracle_bsk, mlk, count):
     got = from_dev(d_out, np.uint64)
     dec = dec_blocks(params, keys, got)
     assert dec == [int(fs[m][x]) for x in msgs for m in range(mlk)]
-    check = np.arange(count) if count <= 8 else np.r_[0:3, 296:count]
+    check = np.arange(count) if count <= 8 else np.r_[0:3, 296:count] if count > 296 else np.r_[0:3, count - 3:count]
     rows = (check[:, None] * mlk + np.arange(mlk)).ravel()
     want = oracle_bsk.ks_pbs(keys["ksk"], ct[check], luts, ids[check], mlk=mlk)
     assert np.array_equal(got[rows], want)
