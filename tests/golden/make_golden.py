@@ -56,7 +56,11 @@ def bitrev(x, bits):
     return int(format(x, "0%db" % bits)[::-1], 2)
 
 
-def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120, ks_bl=3, ks_lc=6, pbs_bl=23):
+RAW_FILES = ["ksk_hwo_0.dat", "glwe_sd_rev.dat", "batch#0/input_blwe_sd_rev.dat",
+             "batch#0/output_blwe_sd_rev.dat", "batch#0/inner_slwe.dat", "batch#0/inner_slwe_2N.dat"]
+
+
+def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120, ks_bl=3, ks_lc=6, pbs_bl=23, keep_raw=False):
     gtv = os.path.join(ref, "sw/bin/gtv/v1.4.1/gtv")
     out = tempfile.mkdtemp(prefix="gtv_")
     lwe_sd, glwe_sd = noise
@@ -100,6 +104,12 @@ def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120, ks_bl=3, ks_lc
         "lut_natural": np.array(lut_nat, np.uint64),
     }
     np.savez_compressed(os.path.join(HERE, f"gtv_{name}.npz"), **fx)
+    if keep_raw:  # the text files themselves, for the file importer's tests
+        import shutil
+        raw = os.path.join(HERE, f"gtv_raw_{name}")
+        os.makedirs(raw, exist_ok=True)
+        for f in RAW_FILES:
+            shutil.copy(os.path.join(d, f), os.path.join(raw, f.replace("batch#0/", "")))
     print(f"gtv_{name}: n={n} N={N} pbs={len(names)} msgs={msgs}")
 
 
@@ -189,7 +199,7 @@ def modswitch_vectors():
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     if "--models-only" not in sys.argv:
-        run_gtv(ref, "n8_N64_noiseless", 8, 64, 4, 7, (0.0, 0.0))
+        run_gtv(ref, "n8_N64_noiseless", 8, 64, 4, 7, (0.0, 0.0), keep_raw=True)
         run_gtv(ref, "n32_N256", 32, 256, 6, 11, (5.3943e-6, 4.4409e-16))
         run_gtv(ref, "n32_N2048", 32, 2048, 3, 13, (5.3943e-6, 4.4409e-16))
         # decompositions of the reference's other parameter sets
