@@ -315,6 +315,20 @@ def cpu_keyswitch(blwe, gpu_out21, ksk, params):
     return res
 
 
+def hbm_peak_gbs():
+    """The HBM copy bandwidth measured on this pool (MEASURED_PEAKS.json, when
+    the file is present), else the pool's earlier measurement, 6650 GB/s."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = json.load(f).get("hbm_gbs")
+        if v:
+            return float(v), "measured (MEASURED_PEAKS.json)"
+    except (OSError, ValueError):
+        pass
+    return 6650.0, "fallback (earlier measurement on this pool)"
+
+
 def br_launches_per_step(B, nsm, g):
     """Blind-rotation launches of one KS+PBS call (luthe_b200/csrc/kernels.cu,
     launch_blind_rotate): one, or two when a partial last wave of at most one
@@ -516,11 +530,15 @@ def main():
     ks_ms = timed(lambda: eng.keyswitch(ks_in, ks_o21, ks_o2n, 16384, stream))
     ks_sample = (ks_in[:64].cpu().numpy().view(np.uint64), ks_o21[:64].cpu().numpy().view(np.uint32))
     del ks_in, ks_o21, ks_o2n
+    hbm_peak, hbm_src = hbm_peak_gbs()
     other = {
         "ntt_product_4096_pairs": {
             "ms": ntt_ms, "pairs_per_s": 4096 / (ntt_ms * 1e-3),
             "modmul_per_s": 4096 * 35840 / (ntt_ms * 1e-3),
             "hbm_gbs_algorithmic": 4096 * 3 * 2048 * 8 / (ntt_ms * 1e-3) / 1e9,
+            "hbm_frac": 4096 * 3 * 2048 * 8 / (ntt_ms * 1e-3) / 1e9 / hbm_peak, "hbm_peak_gbs": hbm_peak,
+            "hbm_peak_source": hbm_src,
+            "imad_frac_of_measured_peak": 4096 * 35840 * IMAD_PER_MODMUL / (ntt_ms * 1e-3) / imad_peak,
             "note": "N=2048 pairs, uniform in [0,2^62); 3 transforms + product per pair"},
         "keyswitch_16384": {
             "ms": ks_ms, "ciphertexts_per_s": 16384 / (ks_ms * 1e-3),
