@@ -194,7 +194,11 @@ int luthe_autotune(luthe_ctx *ctx, size_t sample, char *json, size_t json_cap);
  * (sticky, cleared by this call; the stream must have been synchronised):
  * LUTHE_E_TIMEOUT when a bounded wait for a BSK slab ran out, LUTHE_E_PARAM
  * when a device-resident LUT id was >= the uploaded LUT count (that
- * ciphertext was rotated against LUT 0; its output is not meaningful). */
+ * ciphertext was rotated against LUT 0; its output is not meaningful).  A
+ * timeout whose block could not confirm, within a second bound, that its last
+ * slab copy had finished landing in shared memory is also LUTHE_E_TIMEOUT,
+ * with a message saying that the device state is unsafe: destroy the context
+ * and end the process before using the device again. */
 int luthe_check_device_error(luthe_ctx *ctx);
 
 /* Integer-pipe peaks of `device` measured by probe kernels: 32-bit IMAD per

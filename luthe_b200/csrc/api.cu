@@ -5,6 +5,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <stdarg.h>
+#include <atomic>
 #include <string>
 #include <vector>
 #include "../../include/luthe.h"
@@ -412,6 +413,11 @@ extern "C" int luthe_check_device_error(luthe_ctx *c)
     CUDA_TRY(cudaMemcpy(&e, c->d_err, 4, cudaMemcpyDeviceToHost));
     if (e) {
         cudaMemset(c->d_err, 0, 4);
+        if (e & DEVERR_DRAIN)
+            return fail(LUTHE_E_TIMEOUT,
+                        "blind rotation: a bounded wait ran out and a BSK copy still in flight did not finish "
+                        "landing in shared memory; the device state is unsafe: destroy this context and "
+                        "end the process before further use of the device");
         if (e & DEVERR_TIMEOUT)
             return fail(LUTHE_E_TIMEOUT, "blind rotation: bounded wait for a BSK slab ran out%s",
                         (e & DEVERR_LUT_ID) ? " (and a LUT id was out of range)" : "");
@@ -526,9 +532,11 @@ static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_SCRATCH_WORD
 
 // In host code g_noalloc_scratch names a host-side stand-in, not device memory:
 // the kernels get the device address, looked up once per device with that
-// device current.
-static uint32_t *g_noalloc_addr[64];
-static bool g_noalloc_ready[64];
+// device current.  The per-device address is published with release/acquire
+// ordering, so host threads making their first calls at the same time (on one
+// device or on several) either see the full address or look it up again; a
+// repeated lookup returns the same address.
+static std::atomic<uint32_t *> g_noalloc_addr[64];
 
 extern "C" int luthe_ks_pbs_noalloc(luthe_ctx *c, const uint64_t *d_in, const uint32_t *d_ids, uint64_t *d_out,
                                     size_t count, void *stream)
@@ -543,13 +551,14 @@ extern "C" int luthe_ks_pbs_noalloc(luthe_ctx *c, const uint64_t *d_in, const ui
                     count, NOALLOC_SCRATCH_WORDS / n1, c->p.lwe_dim);
     if (c->device < 0 || c->device >= 64) return fail(LUTHE_E_PARAM, "device index %d out of range", c->device);
     CUDA_TRY(cudaSetDevice(c->device));
-    if (!g_noalloc_ready[c->device]) {
+    uint32_t *scratch = g_noalloc_addr[c->device].load(std::memory_order_acquire);
+    if (!scratch) {
         void *addr = nullptr;
         CUDA_TRY(cudaGetSymbolAddress(&addr, g_noalloc_scratch));
-        g_noalloc_addr[c->device] = (uint32_t *)addr;
-        g_noalloc_ready[c->device] = true;
+        if (!addr) return fail(LUTHE_E_CUDA, "luthe_ks_pbs_noalloc: no device address for the fixed scratch");
+        scratch = (uint32_t *)addr;
+        g_noalloc_addr[c->device].store(scratch, std::memory_order_release);
     }
-    uint32_t *scratch = g_noalloc_addr[c->device];
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t n = c->p.lwe_dim;
     CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, scratch, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level));

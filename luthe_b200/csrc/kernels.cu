@@ -628,7 +628,8 @@ __global__ void __launch_bounds__(G * 256, 1)
         if (*failed) {  // read by every thread after the barrier: uniform
             // the last slab issued may still be landing in this block's shared
             // memory: wait for it (bounded) before the block ends
-            if (threadIdx.x == 0) mbar_wait(mbar, *last_parity, DRAIN_POLLS);
+            if (threadIdx.x == 0 && !mbar_wait(mbar, *last_parity, DRAIN_POLLS))
+                atomicOr(err, DEVERR_DRAIN);  // a copy may still land in shared memory
             return;
         }
     }
@@ -760,7 +761,8 @@ __global__ void __launch_bounds__(512, 1)
         if (!ok) {        // the block agreed on the timeout above
             if (threadIdx.x == 0) {
                 atomicOr(err, DEVERR_TIMEOUT);
-                mbar_wait(mbar, *last_parity, DRAIN_POLLS);  // a slab still landing here
+                if (!mbar_wait(mbar, *last_parity, DRAIN_POLLS))  // a slab still landing here
+                    atomicOr(err, DEVERR_DRAIN);
             }
             return;
         }
@@ -963,7 +965,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     }
     if (!ok && t == 0) {
         if (r == 0) atomicOr(err, DEVERR_TIMEOUT);
-        mbar_wait(mbar, *last_parity, DRAIN_POLLS);  // a half slab still landing here
+        if (!mbar_wait(mbar, *last_parity, DRAIN_POLLS))  // a half slab still landing here
+            atomicOr(err, DEVERR_DRAIN);
     }
     cluster.sync();  // no CTA leaves while the other may still address its shared memory
 }

@@ -54,6 +54,7 @@ constexpr int LWE_COPY = 7;
 // device error flag bits (luthe_check_device_error)
 constexpr uint32_t DEVERR_TIMEOUT = 1u;  // a bounded wait for a BSK slab ran out
 constexpr uint32_t DEVERR_LUT_ID = 2u;   // a LUT id >= the uploaded LUT count
+constexpr uint32_t DEVERR_DRAIN = 4u;    // after a timeout, a slab copy in flight did not finish landing
 struct AluOp {
     uint32_t op, dst, a, b;
     uint64_t imm;
