@@ -5,13 +5,13 @@ algorithms (each C function cites the reference file it follows).  Only the
 tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use
 this module, as the checker; the engine never does.
 
-Parity pins: the key switch and the LUT/BLWE formats are pinned against the
-reference's own golden vectors (``tests/golden``, made by the reference's
-test-vector generator); the decomposer, monomial multiply, Solinas reduction,
-modulus switch and NTT are pinned against the reference's Python models and
-self-tests.  The full blind rotation is not pinned against the reference's
-vectors (their BSK encoding is undecoded); it is pinned stage by stage and by
-decryption.
+Parity pins: the full KS+PBS (key switch, blind rotation, sample extract)
+equals the reference's test-vector generator's outputs word for word, on its
+own keys and BSK files, with the generator's tie rule (``tests/golden``,
+made by the reference's generator; tests/test_reference_pbs_pin.py); the
+decomposer, monomial multiply, Solinas reduction, modulus switch and NTT are
+also pinned stage by stage against the reference's Python models and
+self-tests.
 """
 import ctypes
 import os
@@ -52,6 +52,10 @@ def lib():
         L.or_keyswitch2.argtypes = [vp, vp, u32, u32, u32, u32, u32, u32, ctypes.c_int, vp, vp]
         L.or_bsk_prepare.argtypes = [vp, u32, u32]
         L.or_bsk_prepare.restype = vp
+        L.or_bsk_prepare_eval.argtypes = [vp, u32, u32]
+        L.or_bsk_prepare_eval.restype = vp
+        L.or_ntt_inv_natural.argtypes = [vp, vp, u32]
+        L.or_set_tie_rule.argtypes = [ctypes.c_int]
         L.or_bsk_free.argtypes = [vp]
         L.or_blind_rotate.argtypes = [vp, vp, vp, vp, vp, u32, u32]
         L.or_ks_pbs.argtypes = [vp, vp, vp, vp, vp, vp, u32, u32, u32, u32, u32]
@@ -102,6 +106,14 @@ def ntt_eval(poly):
     return out
 
 
+def ntt_inv_natural(vals):
+    """Coefficients of A from A(psi^(2k+1)), k in natural order (inverse of ntt_eval)."""
+    vals = np.ascontiguousarray(vals, np.uint64)
+    out = np.zeros_like(vals)
+    lib().or_ntt_inv_natural(_p(vals), _p(out), vals.size)
+    return out
+
+
 def negacyclic_mul(a, b):
     a = np.ascontiguousarray(a, np.uint64)
     b = np.ascontiguousarray(b, np.uint64)
@@ -132,10 +144,13 @@ def keyswitch(blwe, ksk, n, N, ks_bl=3, ks_lc=6, ks_w=21, gtv_top_tie=False):
 class OracleBsk:
     """BSK prepared in the oracle's own NTT domain."""
 
-    def __init__(self, bsk_std_p, n, N):
+    def __init__(self, bsk_std_p, n, N, eval_domain=False):
+        """bsk_std_p: [n][row][col][N] over Z_p, standard domain; or, with
+        eval_domain, the evaluations BSK_i[row][col](psi^(2k+1)) in natural k."""
         self._bsk = np.ascontiguousarray(bsk_std_p, np.uint64)
         self.n, self.N = n, N
-        self.h = lib().or_bsk_prepare(_p(self._bsk), n, N)
+        prep = lib().or_bsk_prepare_eval if eval_domain else lib().or_bsk_prepare
+        self.h = prep(_p(self._bsk), n, N)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -160,6 +175,13 @@ class OracleBsk:
         lib().or_ks_pbs_ml(self.h, _p(ksk), _p(blwe_in), _p(luts), _p(lut_ids), _p(out), blwe_in.shape[0], ks_bl,
                            ks_lc, ks_w, pbs_bl, mlk)
         return out
+
+
+def set_tie_rule(generator):
+    """Tie rule of the decompositions in every later blind rotation and
+    KS+PBS of the oracle: the RTL's (False) or the reference generator's
+    (True).  keyswitch() takes its rule as an argument instead."""
+    lib().or_set_tie_rule(int(bool(generator)))
 
 
 def set_threads(t):

@@ -53,16 +53,21 @@ typedef unsigned __int128 u128;
 
 /* ---------------------------------------------------------------- Goldilocks */
 
+/* The carry and borrow corrections below are written as masks rather than
+ * branches: the conditions are data-dependent coin flips, and branch-free code
+ * runs several times faster on the host.  The arithmetic is unchanged. */
+static inline uint64_t mask_if(int c) { return (uint64_t)0 - (uint64_t)(c != 0); }
+
 uint64_t or_gl_reduce128(uint64_t lo, uint64_t hi)
 {
     /* x = lo + 2^64 (h0 + 2^32 h1) = lo - h1 + h0 (2^32 - 1)  (mod p) */
     uint64_t h0 = hi & 0xFFFFFFFFull, h1 = hi >> 32;
     uint64_t t = lo - h1;
-    if (lo < h1) t -= GL_EPS;             /* borrow: -2^64 = -(2^32-1) */
+    t -= mask_if(lo < h1) & GL_EPS;       /* borrow: -2^64 = -(2^32-1) */
     uint64_t u = (h0 << 32) - h0;         /* h0 (2^32-1) < 2^64 */
     uint64_t r = t + u;
-    if (r < t) r += GL_EPS;               /* carry: +2^64 = +(2^32-1) */
-    if (r >= GL_P) r -= GL_P;
+    r += mask_if(r < t) & GL_EPS;         /* carry: +2^64 = +(2^32-1) */
+    r -= mask_if(r >= GL_P) & GL_P;
     return r;
 }
 
@@ -71,18 +76,20 @@ static inline uint64_t gl_mul(uint64_t a, uint64_t b)
     u128 x = (u128)a * b;
     return or_gl_reduce128((uint64_t)x, (uint64_t)(x >> 64));
 }
+/* a, b < p */
 static inline uint64_t gl_add(uint64_t a, uint64_t b)
 {
     uint64_t s = a + b;
-    if (s < a) s += GL_EPS;
-    if (s >= GL_P) s -= GL_P;
+    s += mask_if(s < a) & GL_EPS;
+    s -= mask_if(s >= GL_P) & GL_P;
     return s;
 }
 static inline uint64_t gl_sub(uint64_t a, uint64_t b)
 {
     uint64_t d = a - b;
-    if (a < b) d -= GL_EPS;
-    return d >= GL_P ? d - GL_P : d;
+    d -= mask_if(a < b) & GL_EPS;
+    d -= mask_if(d >= GL_P) & GL_P;
+    return d;
 }
 static uint64_t gl_pow(uint64_t a, uint64_t e)
 {
@@ -259,6 +266,17 @@ void or_ntt_eval(const uint64_t *in, uint64_t *out, uint32_t N)
     ntt_free(&t);
 }
 
+/* Coefficients from evaluations: in[k] = A(psi^{2k+1}) in natural k order
+ * (the inverse of or_ntt_eval, including 1/N). */
+void or_ntt_inv_natural(const uint64_t *in, uint64_t *out, uint32_t N)
+{
+    or_ntt_t t;
+    ntt_init(&t, N);
+    for (uint32_t k = 0; k < N; k++) out[bitrev(k, t.logN)] = in[k] % GL_P;
+    ntt_inv(&t, out);
+    ntt_free(&t);
+}
+
 /* Negacyclic product mod (X^N+1, p) of `count` pairs, via NTT. */
 void or_negacyclic_mul(const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t N, uint32_t count)
 {
@@ -360,6 +378,19 @@ void *or_bsk_prepare(const uint64_t *bsk_std_p, uint32_t n, uint32_t N)
     for (long i = 0; i < (long)n * 4; i++) ntt_fwd(&k->ntt, k->bsk_hat + (size_t)i * N);
     return k;
 }
+/* Prepare the BSK from the evaluation domain: bsk_eval[i][row][col][k] =
+ * BSK_i[row][col](psi^{2k+1}), natural k order (values < p). */
+void *or_bsk_prepare_eval(const uint64_t *bsk_eval, uint32_t n, uint32_t N)
+{
+    or_bsk_t *k = calloc(1, sizeof(*k));
+    k->n = n;
+    k->N = N;
+    ntt_init(&k->ntt, N);
+    k->bsk_hat = malloc((size_t)n * 4 * N * 8);
+    for (size_t q = 0; q < (size_t)n * 4; q++)
+        for (uint32_t j = 0; j < N; j++) k->bsk_hat[q * N + bitrev(j, k->ntt.logN)] = bsk_eval[q * N + j] % GL_P;
+    return k;
+}
 void or_bsk_free(void *h)
 {
     or_bsk_t *k = h;
@@ -367,6 +398,12 @@ void or_bsk_free(void *h)
     free(k->bsk_hat);
     free(k);
 }
+
+/* Tie rule of the decompositions of the full path (blind rotation, and the
+ * key switch of or_ks_pbs_ml): 0 the RTL's, 1 the reference generator's; set
+ * for the whole oracle.  See or_decompose2. */
+static int or_tie_gen = 0;
+void or_set_tie_rule(int gen) { or_tie_gen = gen; }
 
 /* One blind rotation + sample extract.  lwe2N: n masks then the body, in [0,2N).
  * lut: GLWE (mask poly, body poly).  out: BLWE, N mask coefs then body. */
@@ -384,7 +421,7 @@ static void br_one(const or_bsk_t *k, const uint32_t *lwe2N, const uint64_t *lut
             or_monomial(acc + t * N, a, rot + t * N, N);
             for (uint32_t j = 0; j < N; j++) {
                 uint64_t dv = rot[t * N + j] - acc[t * N + j];
-                or_decompose(dv, pbs_bl, 1, &dig);
+                or_decompose2(dv, pbs_bl, 1, or_tie_gen, &dig);
                 dh[t * N + j] = dig >= 0 ? (uint64_t)dig : GL_P - (uint64_t)(-(int64_t)dig);
             }
             ntt_fwd(&k->ntt, dh + t * N);
@@ -448,8 +485,8 @@ void or_ks_pbs_ml(void *bsk, const uint32_t *ksk, const uint64_t *blwe_in, const
         uint32_t *o21 = malloc(4 * (n + 1));
 #pragma omp for schedule(static)
         for (long c = 0; c < (long)B; c++)
-            or_keyswitch(blwe_in + (size_t)c * (N + 1), ksk, n, N, ks_bl, ks_lc, ks_w, N, o21,
-                         l2n + (size_t)c * (n + 1));
+            or_keyswitch2(blwe_in + (size_t)c * (N + 1), ksk, n, N, ks_bl, ks_lc, ks_w, N, or_tie_gen, o21,
+                          l2n + (size_t)c * (n + 1));
         free(o21);
     }
     or_blind_rotate_ml(bsk, l2n, luts, lut_id, blwe_out, B, pbs_bl, mlk);

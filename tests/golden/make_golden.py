@@ -1,23 +1,23 @@
 """Generate the golden fixtures of tests/golden from the reference itself.
 
-Run from the repository root, with the reference project checked out at
-REF (default /root/reference):
+Run from the repository root with the path of the reference project checkout:
 
-    python tests/golden/make_golden.py [REF]
+    python tests/golden/make_golden.py REF [--models-only]
 
 Sources (all run, none copied):
   * sw/bin/gtv/v1.4.1/gtv        -- the reference's test-vector generator
-                                    (keys, BLWE in/out, KS outputs, LUT GLWE)
+                                    (keys, BLWE in/out, KS outputs, LUT GLWE, BSK)
   * sw/decomposer/balanced_decomp_unfix_sign_round_bit.py  (hw_decompose)
   * sw/monomial_mult/monomial_mult.py                      (definition)
   * sw/solinas/solinas.py                                  (compute_modulo)
 
-gtv's text outputs are 512-bit hex lines with words packed right to left and
-'X' padding; the layouts decoded here are:
-  ksk_hwo_0.dat (one channel, lbx=lby=lbz=1): u32, index (x*kN + y)*L + z
-  batch#/input_blwe_sd_rev.dat, output_blwe_sd_rev.dat: u64, mask natural, body last
-  batch#/inner_slwe.dat (21-bit), inner_slwe_2N.dat (log2(2N)-bit): u32, n+1 words
-  glwe_sd_rev.dat: u64, mask poly then body poly, coefficients in bit-reversed order
+gtv's text files are read by luthe_b200.hpu_files (format and layouts in its
+docstring).  The arrays of the .npz fixtures keep the files' own coefficient
+order (BLWE masks bit-reversed, KSK mask index in the same order); the
+decoded LUT is stored in natural order.  For the runs marked keep_bsk the
+generator's BSK file itself is kept, gzipped, beside the fixture
+(gtv_raw_<name>/bsk_nd_hwo_0.dat.gz), with the NTT network parameters it was
+written for in the fixture (ntt_psi, ntt_delta; radix 2).
 """
 import contextlib
 import io
@@ -31,25 +31,9 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from luthe_b200.hpu_files import read_sections  # noqa: E402
 P = 2**64 - 2**32 + 1
-
-
-def read_words(path, w):
-    secs, cur, nh = {}, None, w // 4
-    for line in open(path):
-        line = line.strip()
-        if not line:
-            continue
-        if line.startswith("#"):
-            cur = line[1:].strip()
-            secs[cur] = []
-            continue
-        if cur is None:
-            cur = ""
-            secs[cur] = []
-        words = [line[i:i + nh] for i in range(0, len(line), nh)][::-1]
-        secs[cur].extend(int(x, 16) for x in words if "X" not in x)
-    return secs
 
 
 def bitrev(x, bits):
@@ -60,7 +44,15 @@ RAW_FILES = ["ksk_hwo_0.dat", "glwe_sd_rev.dat", "batch#0/input_blwe_sd_rev.dat"
              "batch#0/output_blwe_sd_rev.dat", "batch#0/inner_slwe.dat", "batch#0/inner_slwe_2N.dat"]
 
 
-def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120, ks_bl=3, ks_lc=6, pbs_bl=23, keep_raw=False):
+NTT_PSI, NTT_DELTA = 4, 3  # the generator's --psi / --ntt-delta for every run (radix 2)
+
+
+def read_words(path, w):
+    return {k: [int(x) for x in v] for k, v in read_sections(path, w).items()}
+
+
+def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120, ks_bl=3, ks_lc=6, pbs_bl=23, keep_raw=False,
+            keep_bsk=False):
     gtv = os.path.join(ref, "sw/bin/gtv/v1.4.1/gtv")
     out = tempfile.mkdtemp(prefix="gtv_")
     lwe_sd, glwe_sd = noise
@@ -70,7 +62,7 @@ def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120, ks_bl=3, ks_lc
     cmd = [gtv, "--omega-ru-n", str(phi * phi % P), "--phi-ru-2n", str(phi), "--lwe-dim", str(n), "--glwe-dim", "1", "--poly-size", str(N), "--pbs-bl", str(pbs_bl), "--pbs-lc", "1",
            "--ks-bl", str(ks_bl), "--ks-lc", str(ks_lc), "--ct-w", "64", "--ks-w", "21", "--msg-w", "2", "--carry-w", "2",
            "--pbs-batch", "1", "--pbs-per-batch", str(per_batch), "--seed", str(seed), "--ntt-radix", "2",
-           "--psi", "4", "--ntt-delta", "3", "--lwe-std-dev", repr(lwe_sd), "--glwe-std-dev", repr(glwe_sd),
+           "--psi", str(NTT_PSI), "--ntt-delta", str(NTT_DELTA), "--lwe-std-dev", repr(lwe_sd), "--glwe-std-dev", repr(glwe_sd),
            "--ksk-pc", "1", "--bsk-pc", "1", "--ks-lbx", "1", "--ks-lby", "1", "--ks-lbz", "1",
            "--panic-on-failure", "--verbose", "-o", out]
     log = subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout).stdout
@@ -102,6 +94,7 @@ def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120, ks_bl=3, ks_lc
         "inner_slwe": np.array([s21["SLwe" + k[4:]] for k in names], np.uint32),
         "inner_slwe_2N": np.array([s2n["SLwe2N" + k[4:]] for k in names], np.uint32),
         "lut_natural": np.array(lut_nat, np.uint64),
+        "ntt_psi": NTT_PSI, "ntt_delta": NTT_DELTA,
     }
     np.savez_compressed(os.path.join(HERE, f"gtv_{name}.npz"), **fx)
     if keep_raw:  # the text files themselves, for the file importer's tests
@@ -110,6 +103,13 @@ def run_gtv(ref, name, n, N, per_batch, seed, noise, timeout=120, ks_bl=3, ks_lc
         os.makedirs(raw, exist_ok=True)
         for f in RAW_FILES:
             shutil.copy(os.path.join(d, f), os.path.join(raw, f.replace("batch#0/", "")))
+    if keep_bsk:  # the generator's BSK file, for the importer and the full-PBS pins
+        import gzip
+        raw = os.path.join(HERE, f"gtv_raw_{name}")
+        os.makedirs(raw, exist_ok=True)
+        with open(os.path.join(d, "bsk_nd_hwo_0.dat"), "rb") as src, \
+                gzip.GzipFile(os.path.join(raw, "bsk_nd_hwo_0.dat.gz"), "wb", mtime=0) as dst:
+            dst.write(src.read())
     print(f"gtv_{name}: n={n} N={N} pbs={len(names)} msgs={msgs}")
 
 
@@ -197,16 +197,20 @@ def modswitch_vectors():
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    if len(args) != 1:
+        sys.exit("usage: python tests/golden/make_golden.py REF [--models-only]  (REF: the reference checkout)")
+    ref = args[0]
     if "--models-only" not in sys.argv:
-        run_gtv(ref, "n8_N64_noiseless", 8, 64, 4, 7, (0.0, 0.0), keep_raw=True)
-        run_gtv(ref, "n32_N256", 32, 256, 6, 11, (5.3943e-6, 4.4409e-16))
-        run_gtv(ref, "n32_N2048", 32, 2048, 3, 13, (5.3943e-6, 4.4409e-16))
+        run_gtv(ref, "n8_N64_noiseless", 8, 64, 4, 7, (0.0, 0.0), keep_raw=True, keep_bsk=True)
+        run_gtv(ref, "n32_N256", 32, 256, 6, 11, (5.3943e-6, 4.4409e-16), keep_bsk=True)
+        run_gtv(ref, "n32_N2048", 32, 2048, 3, 13, (5.3943e-6, 4.4409e-16), keep_bsk=True)
         # decompositions of the reference's other parameter sets
-        run_gtv(ref, "n32_N256_ks2x8", 32, 256, 6, 17, (5.3943e-6, 4.4409e-16), ks_bl=2, ks_lc=8)
-        run_gtv(ref, "n32_N256_ks2x7", 32, 256, 6, 19, (5.3943e-6, 4.4409e-16), ks_bl=2, ks_lc=7)
-        run_gtv(ref, "n32_N256_ks3x5", 32, 256, 6, 23, (5.3943e-6, 4.4409e-16), ks_bl=3, ks_lc=5)
-        run_gtv(ref, "n32_N256_ks3x5_pbs22", 32, 256, 6, 29, (5.3943e-6, 4.4409e-16), ks_bl=3, ks_lc=5, pbs_bl=22)
+        run_gtv(ref, "n32_N256_ks2x8", 32, 256, 6, 17, (5.3943e-6, 4.4409e-16), ks_bl=2, ks_lc=8, keep_bsk=True)
+        run_gtv(ref, "n32_N256_ks2x7", 32, 256, 6, 19, (5.3943e-6, 4.4409e-16), ks_bl=2, ks_lc=7, keep_bsk=True)
+        run_gtv(ref, "n32_N256_ks3x5", 32, 256, 6, 23, (5.3943e-6, 4.4409e-16), ks_bl=3, ks_lc=5, keep_bsk=True)
+        run_gtv(ref, "n32_N256_ks3x5_pbs22", 32, 256, 6, 29, (5.3943e-6, 4.4409e-16), ks_bl=3, ks_lc=5, pbs_bl=22,
+                keep_bsk=True)
     decomposer_vectors(ref)
     monomial_vectors(ref)
     solinas_vectors(ref)

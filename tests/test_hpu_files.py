@@ -15,8 +15,13 @@ G = np.load(os.path.join(HERE, "golden", "gtv_n8_N64_noiseless.npz"))
 
 def test_files_decode_to_the_fixture_arrays():
     assert np.array_equal(H.load_ksk(os.path.join(RAW, "ksk_hwo_0.dat")), G["ksk"])
-    assert np.array_equal(H.load_blwes(os.path.join(RAW, "input_blwe_sd_rev.dat")), G["blwe_in"])
-    assert np.array_equal(H.load_blwes(os.path.join(RAW, "output_blwe_sd_rev.dat")), G["blwe_out"])
+    # the fixture arrays keep the file's bit-reversed mask order
+    assert np.array_equal(H.load_blwes(os.path.join(RAW, "input_blwe_sd_rev.dat"), natural=False), G["blwe_in"])
+    assert np.array_equal(H.load_blwes(os.path.join(RAW, "output_blwe_sd_rev.dat"), natural=False), G["blwe_out"])
+    nat = H.load_blwes(os.path.join(RAW, "input_blwe_sd_rev.dat"))
+    N = int(G["N"])
+    assert np.array_equal(nat[:, N], G["blwe_in"][:, N])
+    assert np.array_equal(nat[:, H.bitrev_perm(N)], G["blwe_in"][:, :N])
     assert np.array_equal(H.load_slwes(os.path.join(RAW, "inner_slwe.dat")), G["inner_slwe"])
     assert np.array_equal(H.load_slwes(os.path.join(RAW, "inner_slwe_2N.dat")), G["inner_slwe_2N"])
     luts = H.load_glwes(os.path.join(RAW, "glwe_sd_rev.dat"), int(G["N"]))
@@ -31,6 +36,33 @@ def test_imported_lut_is_the_engines_lut():
 
 def test_blwe_file_round_trip_is_byte_identical(tmp_path):
     src = os.path.join(RAW, "input_blwe_sd_rev.dat")
-    out = tmp_path / "blwe.dat"
-    H.write_blwes(out, H.load_blwes(src))
-    assert open(out).read().split() == open(src).read().split()
+    for natural in (True, False):
+        out = tmp_path / f"blwe_{natural}.dat"
+        H.write_blwes(out, H.load_blwes(src, natural=natural), natural=natural)
+        assert open(out).read().split() == open(src).read().split()
+
+
+def test_ksk_natural_order_matches_natural_ciphertexts():
+    """A key switch gives the same result with (file-order KSK, file-order
+    BLWE) and with both converted to natural order."""
+    import oracle
+    n, N, L = int(G["n"]), int(G["N"]), int(G["ks_lc"])
+    ksk_nat = H.load_ksk(os.path.join(RAW, "ksk_hwo_0.dat"), N=N, levels=L)
+    nat = H.load_blwes(os.path.join(RAW, "input_blwe_sd_rev.dat"))
+    for c in range(nat.shape[0]):
+        a = oracle.keyswitch(G["blwe_in"][c], G["ksk"], n, N, 3, L, gtv_top_tie=True)
+        b = oracle.keyswitch(nat[c], ksk_nat, n, N, 3, L, gtv_top_tie=True)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_bsk_loader_checks_its_input():
+    raw = os.path.join(RAW, "bsk_nd_hwo_0.dat.gz")
+    n, N = int(G["n"]), int(G["N"])
+    b = H.load_bsk(raw, n, N, int(G["ntt_psi"]), int(G["ntt_delta"]))
+    assert b.shape == (n, 2, 2, N) and int(b.max()) < 2**64 - 2**32 + 1
+    try:
+        H.load_bsk(raw, n + 1, N, 4, 3)
+    except ValueError:
+        pass
+    else:
+        raise AssertionError("a BSK of the wrong size was accepted")
