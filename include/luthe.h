@@ -97,9 +97,29 @@ uint64_t luthe_device_bytes(const luthe_ctx *ctx);
 
 /* Key material (bsk_manager.sv / ksk_manager.sv: keys resident before BR). */
 int luthe_upload_bsk(luthe_ctx *ctx, const uint64_t *h_bsk_std_p);
+/* The BSK given in the evaluation domain, as the HPU receives it from its
+ * host (hw/module/bsk/module/bsk_manager; the reference generator's
+ * bsk_nd_hwo files, whose AXI order is hw/module/hpu/simu/scripts/
+ * gen_stimuli.py:108-127): index ((i*2 + row)*2 + col)*N + k holds
+ * BSK_i[row][col](psi^(2k+1)) mod p, k in natural order, psi the 2N-th root
+ * of luthe_ntt_fwd.  luthe_b200.hpu_files.load_bsk turns a bsk_nd_hwo file
+ * into this form. */
+int luthe_upload_bsk_eval(luthe_ctx *ctx, const uint64_t *h_bsk_eval);
 int luthe_upload_ksk(luthe_ctx *ctx, const uint32_t *h_ksk);
 /* LUT memory, indexed by the PBS DOp's gid (dflt_cfg.toml:18-19 lut_mem). */
 int luthe_upload_luts(luthe_ctx *ctx, const uint64_t *h_glwe, uint32_t count);
+
+/* Tie rule of both balanced decompositions (key switch, blind rotation) for a
+ * top digit equal to B/2.  LUTHE_TIE_RTL (the default) follows the RTL
+ * (hw/module/decomposer/module/decomp_parallel/rtl/decomp_parallel.sv:73-75,
+ * 142-150): the digit is -B/2 when the rounded value's lower bits or rounding
+ * bit are set.  LUTHE_TIE_GENERATOR follows the reference's test-vector
+ * generator (sw/bin/gtv, built on TFHE-rs): the digit stays +B/2.  Both
+ * decompose to the same value; with the generator's rule and the generator's
+ * keys, outputs equal the generator's output_blwe files word for word. */
+#define LUTHE_TIE_RTL 0
+#define LUTHE_TIE_GENERATOR 1
+int luthe_set_tie_rule(luthe_ctx *ctx, int rule);
 
 /* Pre-size the per-call scratch for batches up to `max_count` ciphertexts, so
  * later calls (and graph captures) allocate nothing. */

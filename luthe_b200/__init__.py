@@ -23,11 +23,14 @@ LIB_PATH = os.path.join(_HERE, "libluthe.so")
 
 OK, E_PARAM, E_BUDGET, E_TIMEOUT, E_CUDA, E_STATE = range(6)
 OP_ADD, OP_SUB, OP_MAC, OP_ADDS, OP_SUBS, OP_SSUB, OP_MULS = range(7)
+# tie rule of the decompositions (luthe_set_tie_rule): the RTL's, or the
+# reference test-vector generator's
+TIE_RTL, TIE_GENERATOR = 0, 1
 
 # exported symbols of include/luthe.h
 SYMBOLS = [
     "luthe_params_default", "luthe_last_error", "luthe_ctx_create", "luthe_ctx_destroy", "luthe_device_bytes",
-    "luthe_upload_bsk", "luthe_upload_ksk", "luthe_upload_luts", "luthe_reserve", "luthe_ks_pbs",
+    "luthe_upload_bsk", "luthe_upload_bsk_eval", "luthe_set_tie_rule", "luthe_upload_ksk", "luthe_upload_luts", "luthe_reserve", "luthe_ks_pbs",
     "luthe_ks_pbs_host", "luthe_ks_pbs_graph", "luthe_ks_pbs_noalloc", "luthe_ks_pbs_ml", "luthe_keyswitch",
     "luthe_server_create", "luthe_server_destroy", "luthe_server_submit", "luthe_server_step",
     "luthe_server_fetch", "luthe_server_counters", "luthe_blind_rotate", "luthe_ntt_fwd",
@@ -73,6 +76,8 @@ def lib():
         L.luthe_device_bytes.argtypes = [vp]
         L.luthe_device_bytes.restype = u64
         L.luthe_upload_bsk.argtypes = [vp, vp]
+        L.luthe_upload_bsk_eval.argtypes = [vp, vp]
+        L.luthe_set_tie_rule.argtypes = [vp, ctypes.c_int]
         L.luthe_upload_ksk.argtypes = [vp, vp]
         L.luthe_upload_luts.argtypes = [vp, vp, u32]
         L.luthe_reserve.argtypes = [vp, sz]
@@ -250,6 +255,17 @@ class Engine:
     def upload_bsk(self, bsk):
         bsk = np.ascontiguousarray(bsk, np.uint64)
         _check(lib().luthe_upload_bsk(self._h, _ptr(bsk)))
+
+    def upload_bsk_eval(self, bsk_eval):
+        """BSK in the evaluation domain, [n][row][col][k] = BSK_i[row][col](psi^(2k+1))
+        (the form hpu_files.load_bsk returns for the HPU's bsk_nd_hwo files)."""
+        bsk_eval = np.ascontiguousarray(bsk_eval, np.uint64)
+        _check(lib().luthe_upload_bsk_eval(self._h, _ptr(bsk_eval)))
+
+    def set_tie_rule(self, rule):
+        """TIE_RTL (default) or TIE_GENERATOR: the decompositions' rule for a top
+        digit equal to B/2 (luthe_set_tie_rule)."""
+        _check(lib().luthe_set_tie_rule(self._h, rule))
 
     def upload_ksk(self, ksk):
         ksk = np.ascontiguousarray(ksk, np.uint32)

@@ -155,6 +155,44 @@ extern "C" int luthe_upload_bsk(luthe_ctx *c, const uint64_t *h)
     return LUTHE_OK;
 }
 
+extern "C" int luthe_upload_bsk_eval(luthe_ctx *c, const uint64_t *h)
+{
+    if (!c || !h) return fail(LUTHE_E_PARAM, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t n = c->p.lwe_dim, words = n * 4 * N;
+    for (size_t i = 0; i < words; i++)
+        if (h[i] >= 0xFFFFFFFF00000001ull) return fail(LUTHE_E_PARAM, "BSK word %zu is not reduced mod p", i);
+    // slab[i][p][row*2+col][t] = N^-1 * BSK_i[row][col](psi^(2k+1)), k = eval_index(t, p):
+    // the layout bsk_prepare_kernel writes from the standard domain
+    const uint64_t n_inv = 0xffdfffff00200001ull;  // 2048^-1 mod p
+    std::vector<uint64_t> slab(words);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)n; i++)
+        for (int pp = 0; pp < 8; pp++)
+            for (int q = 0; q < 4; q++)
+                for (int t = 0; t < 256; t++) {
+                    const int k = (t & 31) + 32 * (t >> 5) + 256 * (((pp & 1) << 2) | (pp & 2) | ((pp >> 2) & 1));
+                    const unsigned __int128 x = (unsigned __int128)h[((size_t)i * 4 + q) * N + k] * n_inv;
+                    slab[(((size_t)i * 8 + pp) * 4 + q) * 256 + t] = (uint64_t)(x % 0xFFFFFFFF00000001ull);
+                }
+    int r;
+    if (!c->d_bsk && (r = dalloc(c, (void **)&c->d_bsk, n * SLAB_BYTES))) return r;
+    CUDA_TRY(cudaMemcpy(c->d_bsk, slab.data(), words * 8, cudaMemcpyHostToDevice));
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_set_tie_rule(luthe_ctx *c, int rule)
+{
+    if (!c) return fail(LUTHE_E_PARAM, "null ctx");
+    if (rule != LUTHE_TIE_RTL && rule != LUTHE_TIE_GENERATOR) return fail(LUTHE_E_PARAM, "unknown tie rule %d", rule);
+    if ((uint32_t)rule != c->tie_rule) {
+        CUDA_TRY(cudaSetDevice(c->device));
+        drop_graphs(c);  // captured launches carry the old rule
+        c->tie_rule = (uint32_t)rule;
+    }
+    return LUTHE_OK;
+}
+
 extern "C" int luthe_upload_ksk(luthe_ctx *c, const uint32_t *h)
 {
     if (!c || !h) return fail(LUTHE_E_PARAM, "null argument");
@@ -222,9 +260,9 @@ static int enqueue_ks_pbs(luthe_ctx *c, const uint64_t *d_in, const uint32_t *d_
                           cudaStream_t s)
 {
     const uint32_t n = c->p.lwe_dim;
-    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level));
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level, c->tie_rule));
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out,
-                                 count, n, c->d_err, s, nullptr, 1, c->p.pbs_base_log));
+                                 count, n, c->d_err, s, nullptr, 1, c->p.pbs_base_log, c->tie_rule));
     return LUTHE_OK;
 }
 
@@ -252,9 +290,9 @@ extern "C" int luthe_ks_pbs_ml(luthe_ctx *c, const uint64_t *d_in, const uint32_
     if ((r = ensure_scratch(c, count))) return r;
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t n = c->p.lwe_dim;
-    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level));
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level, c->tie_rule));
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out, count,
-                                 n, c->d_err, s, nullptr, mlk, c->p.pbs_base_log));
+                                 n, c->d_err, s, nullptr, mlk, c->p.pbs_base_log, c->tie_rule));
     return LUTHE_OK;
 }
 
@@ -336,7 +374,7 @@ extern "C" int luthe_keyswitch(luthe_ctx *c, const uint64_t *d_in, uint32_t *d_o
     if (!d_in || !d_out2N) return fail(LUTHE_E_PARAM, "null buffer");
     CUDA_TRY(cudaSetDevice(c->device));
     CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, d_out21, d_out2N, count, c->p.lwe_dim, c->xpad,
-                              (cudaStream_t)stream, nullptr, c->p.ks_base_log, c->p.ks_level));
+                              (cudaStream_t)stream, nullptr, c->p.ks_base_log, c->p.ks_level, c->tie_rule));
     return LUTHE_OK;
 }
 
@@ -349,7 +387,7 @@ extern "C" int luthe_blind_rotate(luthe_ctx *c, const uint32_t *d_lwe2N, const u
     if (!d_lwe2N || !d_ids || !d_out) return fail(LUTHE_E_PARAM, "null buffer");
     CUDA_TRY(cudaSetDevice(c->device));
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out, count,
-                                 c->p.lwe_dim, c->d_err, (cudaStream_t)stream, nullptr, 1, c->p.pbs_base_log));
+                                 c->p.lwe_dim, c->d_err, (cudaStream_t)stream, nullptr, 1, c->p.pbs_base_log, c->tie_rule));
     return LUTHE_OK;
 }
 
@@ -466,11 +504,11 @@ extern "C" int luthe_autotune(luthe_ctx *c, size_t sample, char *json, size_t ca
         cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
         if ((size_t)max_smem < cfg.ctas_per_sm * (smem + 1024)) continue;
         cudaError_t e = launch_blind_rotate(cfg, c->nsm, d_l, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_o,
-                                            sample, n, c->d_err, 0, nullptr, 1, c->p.pbs_base_log);
+                                            sample, n, c->d_err, 0, nullptr, 1, c->p.pbs_base_log, c->tie_rule);
         cudaEventRecord(e0, 0);
         for (int rep = 0; rep < 2 && e == cudaSuccess; rep++)
             e = launch_blind_rotate(cfg, c->nsm, d_l, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_o, sample, n,
-                                    c->d_err, 0, nullptr, 1, c->p.pbs_base_log);
+                                    c->d_err, 0, nullptr, 1, c->p.pbs_base_log, c->tie_rule);
         cudaEventRecord(e1, 0);
         if (e == cudaSuccess) e = cudaEventSynchronize(e1);
         if (e != cudaSuccess) {
@@ -561,8 +599,8 @@ extern "C" int luthe_ks_pbs_noalloc(luthe_ctx *c, const uint64_t *d_in, const ui
     }
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t n = c->p.lwe_dim;
-    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, scratch, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level));
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, scratch, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level, c->tie_rule));
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, scratch, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out, count, n,
-                                 c->d_err, s, nullptr, 1, c->p.pbs_base_log));
+                                 c->d_err, s, nullptr, 1, c->p.pbs_base_log, c->tie_rule));
     return LUTHE_OK;
 }

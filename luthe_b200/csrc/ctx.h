@@ -34,6 +34,7 @@ struct luthe_ctx {
     uint32_t *d_hids = nullptr;
     size_t hcap = 0;
     luthe::BrConfig br{2, 1};
+    uint32_t tie_rule = luthe::TIE_RTL;  // decomposition tie rule (luthe_set_tie_rule)
     std::vector<GraphEntry> graphs;
 };
 

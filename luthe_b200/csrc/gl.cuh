@@ -259,15 +259,18 @@ __device__ __forceinline__ u64 modsw_p_to_q(u64 a)
 // Balanced decomposition, base 2^23, one level, of a 64-bit torus value,
 // embedded in Z_p (decomp_balseq_core.sv:135-150; the rounding and tie rule of
 // sw/decomposer/balanced_decomp_unfix_sign_round_bit.py:42-101 with bw=23, L=1).
+// tie_rtl = 1 selects the RTL's rule at a tie (t = B/2: negative when the
+// rounding bit is set), tie_rtl = 0 the reference generator's (TFHE-rs: the
+// digit above is 0, so the digit stays +B/2).
 template <int BW>
-__device__ __forceinline__ u64 decomp_to_p(u64 v)
+__device__ __forceinline__ u64 decomp_to_p(u64 v, u64 tie_rtl = 1)
 {
     constexpr u64 B = 1ull << BW, HALF = B >> 1;
     u64 rb = (v >> (63 - BW)) & 1ull;
     u64 c = (v >> (64 - BW)) + rb;      // 0 .. 2^BW
     u64 t = c & (B - 1);
     // with one level the digit above is last_sign * (B-1), last_sign = rb at a tie
-    bool negd = (t > HALF) || (t == HALF && rb);
+    bool negd = (t > HALF) || (t == HALF && (rb & tie_rtl));
     // negative digit t - 2^BW embeds as p - (2^BW - t)
     return negd ? (P - (B - t)) : t;
 }

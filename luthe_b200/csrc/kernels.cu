@@ -237,7 +237,11 @@ cudaError_t launch_ntt_mul(const uint64_t *d_a, const uint64_t *d_b, uint64_t *d
 // on the fly from the 64-bit mask coefficients; 32-bit wrap-around keeps the
 // low 21 bits exact.  KSK is transposed to [y*L+z][x] on upload.  Templated
 // on the decomposition (base 2^BL, L levels) of the reference's parameter sets.
-template <int BL, int L>
+// GEN = false: the RTL's tie rule; GEN = true: the rule of the reference's
+// test-vector generator (TFHE-rs), which takes the digit above the top one as
+// 0, so that a top digit equal to B/2 stays positive.  Both give the same
+// value mod 2^(BL*L); they differ only in that top digit.
+template <int BL, int L, bool GEN>
 __device__ __forceinline__ void ks_decomp(u64 v, int *d)
 {
     // closest_rep = top BL*L bits + round bit; tie rule of
@@ -246,7 +250,7 @@ __device__ __forceinline__ void ks_decomp(u64 v, int *d)
     constexpr u32 MASK = (1u << BL) - 1, HALF = 1u << (BL - 1);
     u32 rb = (u32)(v >> (63 - TOT)) & 1u;
     u32 c = (u32)(v >> (64 - TOT)) + rb;  // 0 .. 2^TOT
-    u32 last_sign = ((c >> (TOT - 1)) & 1u) && ((c & ((1u << (TOT - 1)) - 1)) || rb);
+    u32 last_sign = GEN ? 0u : (((c >> (TOT - 1)) & 1u) && ((c & ((1u << (TOT - 1)) - 1)) || rb));
     u32 carry = 0;
 #pragma unroll
     for (int i = 0; i < L; i++) {
@@ -259,7 +263,7 @@ __device__ __forceinline__ void ks_decomp(u64 v, int *d)
     }
 }
 
-template <int BL, int L>
+template <int BL, int L, bool GEN>
 __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, const u32 *__restrict__ src_idx,
                                                   const u32 *__restrict__ ksk_t, u32 *__restrict__ out21,
                                                   u32 *__restrict__ out2N, u32 B, u32 n, u32 xpad)
@@ -281,7 +285,7 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
     for (u32 y0 = 0; y0 < (u32)N; y0 += KS_KC) {
         {
             int d[L];
-            ks_decomp<BL, L>(in[(size_t)dct_g * (N + 1) + y0 + dy], d);
+            ks_decomp<BL, L, GEN>(in[(size_t)dct_g * (N + 1) + y0 + dy], d);
 #pragma unroll
             for (int z = 0; z < L; z++) dsm[dy * L + z][dct] = d[z];
         }
@@ -329,19 +333,29 @@ bool ks_supported(uint32_t bl, uint32_t L)
     return (bl == 3 && (L == 6 || L == 5)) || (bl == 2 && (L == 8 || L == 7));
 }
 
-cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21, uint32_t *d_out2N,
-                             size_t B, uint32_t n, uint32_t xpad, cudaStream_t s, const uint32_t *d_src_idx,
-                             uint32_t bl, uint32_t L)
+template <bool GEN>
+static cudaError_t launch_keyswitch_rule(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21,
+                                         uint32_t *d_out2N, u32 B, uint32_t n, uint32_t xpad, cudaStream_t s,
+                                         const uint32_t *d_src_idx, uint32_t bl, uint32_t L)
 {
-    if (B == 0) return cudaSuccess;
-    dim3 grid(xpad / KS_BN, (unsigned)((B + KS_BM - 1) / KS_BM));
-    const u32 Bu = (u32)B;
-    if (bl == 3 && L == 6) ks_kernel<3, 6><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, Bu, n, xpad);
-    else if (bl == 3 && L == 5) ks_kernel<3, 5><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, Bu, n, xpad);
-    else if (bl == 2 && L == 8) ks_kernel<2, 8><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, Bu, n, xpad);
-    else if (bl == 2 && L == 7) ks_kernel<2, 7><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, Bu, n, xpad);
+    dim3 grid(xpad / KS_BN, (B + KS_BM - 1) / KS_BM);
+    if (bl == 3 && L == 6) ks_kernel<3, 6, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad);
+    else if (bl == 3 && L == 5) ks_kernel<3, 5, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad);
+    else if (bl == 2 && L == 8) ks_kernel<2, 8, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad);
+    else if (bl == 2 && L == 7) ks_kernel<2, 7, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
+}
+
+cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21, uint32_t *d_out2N,
+                             size_t B, uint32_t n, uint32_t xpad, cudaStream_t s, const uint32_t *d_src_idx,
+                             uint32_t bl, uint32_t L, uint32_t tie_rule)
+{
+    if (B == 0) return cudaSuccess;
+    if (tie_rule == TIE_GENERATOR)
+        return launch_keyswitch_rule<true>(d_in, d_ksk_t, d_out21, d_out2N, (u32)B, n, xpad, s, d_src_idx, bl, L);
+    if (tie_rule != TIE_RTL) return cudaErrorInvalidValue;
+    return launch_keyswitch_rule<false>(d_in, d_ksk_t, d_out21, d_out2N, (u32)B, n, xpad, s, d_src_idx, bl, L);
 }
 
 // ---------------------------------------------------------- blind rotation
@@ -433,7 +447,8 @@ template <int G, int BW>
 __global__ void __launch_bounds__(G * 256, 1)
     br_kernel(const u32 *__restrict__ lwe2N, const u64 *__restrict__ luts, const u32 *__restrict__ lut_id, u32 nlut,
               const u64 *__restrict__ bsk, const u64 *__restrict__ tw, u64 *__restrict__ out, u32 B, u32 n,
-              u32 *__restrict__ err, const u32 *__restrict__ dst_idx, u32 mlk)
+              u32 *__restrict__ err, const u32 *__restrict__ dst_idx, u32 mlk,
+              u32 tie_rule)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     u64 *slab = reinterpret_cast<u64 *>(smem_raw);
@@ -444,6 +459,7 @@ __global__ void __launch_bounds__(G * 256, 1)
     u32 *failed = slab_done + 1;
     u32 *last_parity = failed + 1;  // phase parity of the last slab issued
     const unsigned long long polls = g_slab_wait_polls;
+    const u64 tie_rtl = tie_rule == TIE_RTL ? 1ull : 0ull;
     const int g = threadIdx.x >> 8, t = threadIdx.x & 255, bar = 1 + g;
     // two staging buffers per ciphertext group (fixed roles, see the step below)
     u64 *bp = bufs + g * 4 * POLY_WORDS, *bq = bp + 2 * POLY_WORDS;
@@ -521,7 +537,7 @@ __global__ void __launch_bounds__(G * 256, 1)
                     const u32 src = (j + TWO_N - a) & (TWO_N - 1);
                     u64 v = accq[src & (N - 1)];
                     if (src >= (u32)N) v = 0ull - v;
-                    y[e] = gl::decomp_to_p<BW>(v - accq[j]);
+                    y[e] = gl::decomp_to_p<BW>(v - accq[j], tie_rtl);
                 }
                 ntt::a1_fwd(y, bq + q * POLY_WORDS, t);
             }
@@ -648,7 +664,8 @@ template <int BW>
 __global__ void __launch_bounds__(512, 1)
     br_kernel_split(const u32 *__restrict__ lwe2N, const u64 *__restrict__ luts, const u32 *__restrict__ lut_id,
                     u32 nlut, const u64 *__restrict__ bsk, const u64 *__restrict__ tw, u64 *__restrict__ out, u32 B,
-                    u32 n, u32 *__restrict__ err, const u32 *__restrict__ dst_idx, u32 mlk)
+                    u32 n, u32 *__restrict__ err, const u32 *__restrict__ dst_idx, u32 mlk,
+              u32 tie_rule)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     u64 *slab = reinterpret_cast<u64 *>(smem_raw);
@@ -657,6 +674,7 @@ __global__ void __launch_bounds__(512, 1)
     u64 *mbar = bufs + 4 * POLY_WORDS;
     u32 *last_parity = reinterpret_cast<u32 *>(mbar + 1);  // phase parity of the last slab issued
     const unsigned long long polls = g_slab_wait_polls;
+    const u64 tie_rtl = tie_rule == TIE_RTL ? 1ull : 0ull;
     const int g = threadIdx.x >> 8, t = threadIdx.x & 255, bar = 1 + g;
     u64 *bp = bufs + g * 2 * POLY_WORDS, *bq = bp + POLY_WORDS;  // this group's polynomial
     const u64 *bp0 = bufs, *bp1 = bufs + 2 * POLY_WORDS;          // both groups' bp (MAC operands, extract)
@@ -707,7 +725,7 @@ __global__ void __launch_bounds__(512, 1)
                     const u32 src = (j + TWO_N - a) & (TWO_N - 1);
                     u64 v = bp[src & (N - 1)];
                     if (src >= (u32)N) v = 0ull - v;
-                    y[e] = gl::decomp_to_p<BW>(v - bp[j]);
+                    y[e] = gl::decomp_to_p<BW>(v - bp[j], tie_rtl);
                 }
                 ntt::a1_fwd(y, bq, t);
             }
@@ -821,7 +839,8 @@ template <int BW>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     br_kernel_pair(const u32 *__restrict__ lwe2N, const u64 *__restrict__ luts, const u32 *__restrict__ lut_id,
                    u32 nlut, const u64 *__restrict__ bsk, const u64 *__restrict__ tw, u64 *__restrict__ out, u32 B,
-                   u32 n, u32 *__restrict__ err, const u32 *__restrict__ dst_idx, u32 mlk)
+                   u32 n, u32 *__restrict__ err, const u32 *__restrict__ dst_idx, u32 mlk,
+              u32 tie_rule)
 {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
@@ -834,6 +853,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     u32 *flags = reinterpret_cast<u32 *>(mbar + 1);  // step status of rank 0 and rank 1
     u32 *last_parity = flags + 2;                     // phase parity of the last half slab issued
     const unsigned long long polls = g_slab_wait_polls;
+    const u64 tie_rtl = tie_rule == TIE_RTL ? 1ull : 0ull;
     const int t = threadIdx.x;
     const u64 *peer_bp = cluster.map_shared_rank(bp, r ^ 1u);
     u32 *peer_flags = cluster.map_shared_rank(flags, r ^ 1u);
@@ -884,7 +904,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                     const u32 src = (j + TWO_N - a) & (TWO_N - 1);
                     u64 v = bp[src & (N - 1)];
                     if (src >= (u32)N) v = 0ull - v;
-                    y[e] = gl::decomp_to_p<BW>(v - bp[j]);
+                    y[e] = gl::decomp_to_p<BW>(v - bp[j], tie_rtl);
                 }
                 ntt::a1_fwd(y, bq, t);
             }
@@ -1014,14 +1034,15 @@ cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n)
 static cudaError_t launch_br_once(int G, int ctas_per_sm, int nsm, const uint32_t *d_lwe2N, const uint64_t *d_luts,
                                   const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk,
                                   const uint64_t *d_tw, uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err,
-                                  cudaStream_t s, const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw)
+                                  cudaStream_t s, const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw,
+                                  uint32_t tie_rule)
 {
     if (G == -1) {  // lowest-latency form: a cluster of two CTAs (two SMs) per ciphertext
         size_t pairs = B < (size_t)(nsm / 2) ? B : (size_t)(nsm / 2);
         u32 Bu = (u32)B;
         void *args[] = {(void *)&d_lwe2N, (void *)&d_luts, (void *)&d_lut_id, (void *)&nlut, (void *)&d_bsk,
                         (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err,
-                        (void *)&d_dst_idx, (void *)&mlk};
+                        (void *)&d_dst_idx, (void *)&mlk, (void *)&tie_rule};
         const void *k = pbs_bw == 22 ? (const void *)br_kernel_pair<22> : (const void *)br_kernel_pair<23>;
         return cudaLaunchKernel(k, dim3((unsigned)(2 * pairs)), dim3(TPG), args, PAIR_SMEM_BYTES, s);
     }
@@ -1030,7 +1051,7 @@ static cudaError_t launch_br_once(int G, int ctas_per_sm, int nsm, const uint32_
         u32 Bu = (u32)B;
         void *args[] = {(void *)&d_lwe2N, (void *)&d_luts, (void *)&d_lut_id, (void *)&nlut, (void *)&d_bsk,
                         (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err,
-                        (void *)&d_dst_idx, (void *)&mlk};
+                        (void *)&d_dst_idx, (void *)&mlk, (void *)&tie_rule};
         const void *k = pbs_bw == 22 ? (const void *)br_kernel_split<22> : (const void *)br_kernel_split<23>;
         return cudaLaunchKernel(k, dim3((unsigned)grid), dim3(512), args, br_split_smem_bytes(), s);
     }
@@ -1041,7 +1062,7 @@ static cudaError_t launch_br_once(int G, int ctas_per_sm, int nsm, const uint32_
     u32 Bu = (u32)B;
     void *args[] = {(void *)&d_lwe2N, (void *)&d_luts, (void *)&d_lut_id, (void *)&nlut, (void *)&d_bsk,
                     (void *)&d_tw,    (void *)&d_out,  (void *)&Bu,       (void *)&n,    (void *)&d_err,
-                    (void *)&d_dst_idx, (void *)&mlk};
+                    (void *)&d_dst_idx, (void *)&mlk, (void *)&tie_rule};
     const void *k;
     if (G == 1) k = pbs_bw == 22 ? (const void *)br_kernel<1, 22> : (const void *)br_kernel<1, 23>;
     else if (G == 2) k = pbs_bw == 22 ? (const void *)br_kernel<2, 22> : (const void *)br_kernel<2, 23>;
@@ -1052,11 +1073,12 @@ static cudaError_t launch_br_once(int G, int ctas_per_sm, int nsm, const uint32_
 cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_lwe2N, const uint64_t *d_luts,
                                 const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
                                 uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s,
-                                const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw)
+                                const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw, uint32_t tie_rule)
 {
     if (B == 0) return cudaSuccess;
     if (mlk != 1 && mlk != 2 && mlk != 4 && mlk != 8) return cudaErrorInvalidValue;
     if (!pbs_supported(pbs_bw)) return cudaErrorInvalidValue;
+    if (tie_rule != TIE_RTL && tie_rule != TIE_GENERATOR) return cudaErrorInvalidValue;
     const int G = cfg.cts_per_cta, cps = cfg.ctas_per_sm;
     const size_t wave = (size_t)nsm * cps * G;
     // A batch that fits one ciphertext per SM runs in the latency form (one
@@ -1066,22 +1088,22 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
     auto small_form = [&](size_t count) { return count <= (size_t)(nsm / 2) ? -1 : 0; };
     if (G > 1 && B <= (size_t)nsm)
         return launch_br_once(small_form(B), 1, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n,
-                              d_err, s, d_dst_idx, mlk, pbs_bw);
+                              d_err, s, d_dst_idx, mlk, pbs_bw, tie_rule);
     // A partial last wave of at most one ciphertext per SM runs as its own
     // latency-form launch after the full waves instead of a full G-per-CTA wave.
     const size_t tail = B % wave;
     if (G > 1 && B > wave && tail > 0 && tail <= (size_t)nsm) {
         const size_t full = B - tail;
         cudaError_t e = launch_br_once(G, cps, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, full, n,
-                                       d_err, s, d_dst_idx, mlk, pbs_bw);
+                                       d_err, s, d_dst_idx, mlk, pbs_bw, tie_rule);
         if (e != cudaSuccess) return e;
         uint64_t *out_tail = d_dst_idx ? d_out : d_out + full * mlk * (size_t)(N + 1);
         return launch_br_once(small_form(tail), 1, nsm, d_lwe2N + full * (size_t)(n + 1), d_luts, d_lut_id + full,
                               nlut, d_bsk, d_tw, out_tail, tail, n, d_err, s, d_dst_idx ? d_dst_idx + full : nullptr,
-                              mlk, pbs_bw);
+                              mlk, pbs_bw, tie_rule);
     }
     return launch_br_once(G, cps, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n, d_err, s,
-                          d_dst_idx, mlk, pbs_bw);
+                          d_dst_idx, mlk, pbs_bw, tie_rule);
 }
 
 // ---------------------------------------------------------- linear DOps

@@ -33,9 +33,13 @@ cudaError_t launch_ntt_inv(const uint64_t *d_in, uint64_t *d_out, const uint64_t
                            cudaStream_t s);
 cudaError_t launch_ntt_mul(const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, const uint64_t *d_tw,
                            size_t count, cudaStream_t s);
+// Tie rule of the balanced decompositions for a top digit equal to B/2:
+// the RTL's (decomp_parallel.sv) or the reference's test-vector generator's.
+constexpr uint32_t TIE_RTL = 0, TIE_GENERATOR = 1;
 cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21, uint32_t *d_out2N,
                              size_t B, uint32_t n, uint32_t xpad, cudaStream_t s,
-                             const uint32_t *d_src_idx = nullptr, uint32_t bl = KS_BL, uint32_t L = KS_L);
+                             const uint32_t *d_src_idx = nullptr, uint32_t bl = KS_BL, uint32_t L = KS_L,
+                             uint32_t tie_rule = TIE_RTL);
 bool ks_supported(uint32_t bl, uint32_t L);
 bool pbs_supported(uint32_t bw);
 // Bound on the polls of each BSK-slab wait of the blind rotation on the
@@ -44,7 +48,8 @@ cudaError_t set_slab_wait_polls(unsigned long long polls);
 cudaError_t launch_blind_rotate(const BrConfig &cfg, int num_sms, const uint32_t *d_lwe2N, const uint64_t *d_luts,
                                 const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
                                 uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s,
-                                const uint32_t *d_dst_idx = nullptr, uint32_t mlk = 1, uint32_t pbs_bw = 23);
+                                const uint32_t *d_dst_idx = nullptr, uint32_t mlk = 1, uint32_t pbs_bw = 23,
+                                uint32_t tie_rule = TIE_RTL);
 size_t br_smem_bytes(const BrConfig &cfg, uint32_t n);
 cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n);
 

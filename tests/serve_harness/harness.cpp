@@ -57,14 +57,14 @@ cudaError_t launch_alu_batch(const AluOp *ops, uint64_t *pool, uint32_t nops, ui
     return cudaSuccess;
 }
 cudaError_t launch_keyswitch(const uint64_t *in, const uint32_t *, uint32_t *, uint32_t *out2N, size_t B, uint32_t n,
-                             uint32_t, cudaStream_t, const uint32_t *src_idx, uint32_t, uint32_t)
+                             uint32_t, cudaStream_t, const uint32_t *src_idx, uint32_t, uint32_t, uint32_t)
 {
     for (size_t c = 0; c < B; c++) out2N[c * (n + 1)] = (uint32_t)in[(size_t)(src_idx ? src_idx[c] : c) * g_w];
     return cudaSuccess;
 }
 cudaError_t launch_blind_rotate(const BrConfig &, int, const uint32_t *l2n, const uint64_t *luts, const uint32_t *ids,
                                 uint32_t, const uint64_t *, const uint64_t *, uint64_t *out, size_t B, uint32_t n,
-                                uint32_t *, cudaStream_t, const uint32_t *dst_idx, uint32_t mlk, uint32_t)
+                                uint32_t *, cudaStream_t, const uint32_t *dst_idx, uint32_t mlk, uint32_t, uint32_t)
 {
     for (size_t c = 0; c < B; c++) {
         const uint32_t x = l2n[c * (n + 1)];

@@ -107,8 +107,8 @@ def _msgs_luts(params, rng, count, nlut):
 # On 148 SMs with two ciphertexts per CTA: 1 and 5 run one ciphertext per two
 # SMs (cluster pairs); 100 one per SM (polynomials split over the CTA's
 # groups); 301 = one full wave + a 5-ciphertext tail in cluster pairs; 450 =
-# one full wave + a partial two-per-CTA wave of 154.  The oracle checks the
-# first ciphertexts and the ciphertexts after the first wave.
+# one full wave + a partial two-per-CTA wave of 154.  The oracle checks every
+# ciphertext.
 @pytest.mark.parametrize("count", [1, 5, 100, 301, 450])
 def test_ks_pbs_bit_exact_and_decrypts(engine, params, keys, oracle_bsk, count):
     rng = np.random.default_rng(60 + count)
@@ -123,9 +123,63 @@ def test_ks_pbs_bit_exact_and_decrypts(engine, params, keys, oracle_bsk, count):
     got = from_dev(d_out, np.uint64)
     dec = L.decrypt(params, keys["glwe_key"], got)
     assert [int(d) for d in dec] == [int(tables[i][m]) for i, m in zip(ids, msgs)]
-    check = np.arange(count) if count <= 8 else np.r_[0:4, 296:count] if count > 296 else np.r_[0:4, count - 4:count]
-    want = oracle_bsk.ks_pbs(keys["ksk"], ct[check], luts, ids[check])
-    assert np.array_equal(got[check], want)
+    want = oracle_bsk.ks_pbs(keys["ksk"], ct, luts, ids)
+    assert np.array_equal(got, want)
+
+
+# The batch sizes of the benchmark's batched configuration (1, 17, 256, 1000,
+# 4096 BLWEs, each batch with its own LUT), each as its own call, every
+# ciphertext checked against the oracle.  On 148 SMs: 17 runs in cluster
+# pairs, 256 as one partial two-per-CTA wave, 1000 as three waves and a
+# 112-ciphertext tail of one per SM, 4096 as thirteen waves and a partial one.
+def test_configured_batch_sizes_bit_exact(engine, params, keys, oracle_bsk):
+    rng = np.random.default_rng(65)
+    engine.set_br_config(2, 1)
+    for count in (17, 256, 1000, 4096):
+        msgs, tables, luts = _msgs_luts(params, rng, count, 1)
+        ids = np.zeros(count, np.uint32)
+        ct = L.encrypt(params, keys["glwe_key"], msgs, 2000 + count)
+        engine.upload_luts(luts)
+        d_out = to_dev(np.zeros_like(ct))
+        engine.ks_pbs(to_dev(ct), to_dev(ids), d_out, count)
+        engine.check_device_error()
+        got = from_dev(d_out, np.uint64)
+        want = oracle_bsk.ks_pbs(keys["ksk"], ct, luts, ids)
+        assert np.array_equal(got, want), f"batch of {count}: rows {np.nonzero((got != want).any(1))[0][:8]}"
+
+
+def test_generator_tie_rule_matches_oracle(engine, params, keys, oracle_bsk):
+    """With the reference generator's tie rule (luthe_set_tie_rule) the engine
+    equals the oracle in the same rule on every ciphertext, across a wave and
+    a tail launch: about one bootstrap in three at n = 804 meets a tie in its
+    blind rotation, and nearly every one in its key switch."""
+    rng = np.random.default_rng(67)
+    count = 301
+    msgs, tables, luts = _msgs_luts(params, rng, count, 2)
+    ids = rng.integers(0, 2, count).astype(np.uint32)
+    ct = L.encrypt(params, keys["glwe_key"], msgs, 2301)
+    engine.upload_luts(luts)
+    engine.set_br_config(2, 1)
+    d_in, d_ids = to_dev(ct), to_dev(ids)
+    d_rtl, d_gen = to_dev(np.zeros_like(ct)), to_dev(np.zeros_like(ct))
+    engine.ks_pbs(d_in, d_ids, d_rtl, count)
+    engine.set_tie_rule(L.TIE_GENERATOR)
+    try:
+        engine.ks_pbs(d_in, d_ids, d_gen, count)
+        engine.check_device_error()
+    finally:
+        engine.set_tie_rule(L.TIE_RTL)
+    got = from_dev(d_gen, np.uint64)
+    oracle.set_tie_rule(True)
+    try:
+        want = oracle_bsk.ks_pbs(keys["ksk"], ct, luts, ids)
+    finally:
+        oracle.set_tie_rule(False)
+    assert np.array_equal(got, want)
+    rtl = from_dev(d_rtl, np.uint64)
+    assert (rtl != got).any(1).sum() > count // 2  # the rules differ in the ciphertexts
+    dec = L.decrypt(params, keys["glwe_key"], got)
+    assert [int(d) for d in dec] == [int(tables[i][m]) for i, m in zip(ids, msgs)]
 
 
 def test_ks_pbs_host_and_graph(engine, params, keys, oracle_bsk):
