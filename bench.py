@@ -127,14 +127,36 @@ def read_traffic(B):
     return small["dram_bytes_fixed_per_launch"] + small["dram_bytes_per_bootstrap"] * B, "ncu, scaled from 296"
 
 
+class _OracleHost:
+    """The host helpers the workload needs, from the oracle's own C code (the
+    same values as the engine library's for the same seed), so that the CPU
+    reference arm loads nothing from the engine library."""
+
+    def __init__(self, oracle):
+        self.o = oracle
+
+    def lut_build(self, params, table):
+        return self.o.lut_build(params.poly_size, table)
+
+    def encrypt(self, params, glwe_key, msgs, seed):
+        return self.o.encrypt(glwe_key, msgs, seed)
+
+    def decrypt(self, params, glwe_key, blwe):
+        return self.o.decrypt(glwe_key, blwe)
+
+
+class _Params:
+    lwe_dim, poly_size = 804, 2048
+
+
 def reference_arm(args):
     import oracle
-    import luthe_b200 as L
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    params = L.default_params()
-    keys = L.keygen(params, args.seed)
+    L = _OracleHost(oracle)
+    params = _Params()
+    keys = oracle.keygen(params.lwe_dim, params.poly_size, args.seed)
     ct, ids, luts, expect = workload(L, params, keys, args.seed)
     ob = oracle.OracleBsk(keys["bsk"], params.lwe_dim, params.poly_size)
     threads = os.cpu_count() or 1

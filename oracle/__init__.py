@@ -60,6 +60,10 @@ def lib():
         L.or_blind_rotate.argtypes = [vp, vp, vp, vp, vp, u32, u32]
         L.or_ks_pbs.argtypes = [vp, vp, vp, vp, vp, vp, u32, u32, u32, u32, u32]
         L.or_ks_pbs_ml.argtypes = [vp, vp, vp, vp, vp, vp, u32, u32, u32, u32, u32, u32]
+        L.or_keygen.argtypes = [u32, u32, u32, u32, u32, u32, u64, vp, vp, vp, vp]
+        L.or_encrypt.argtypes = [u32, u32, vp, vp, u64, u64, vp]
+        L.or_decrypt.argtypes = [u32, u32, vp, vp, u64, vp]
+        L.or_lut_build.argtypes = [u32, u32, vp, vp]
         L.or_num_threads.restype = ctypes.c_int
         L.or_set_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -182,6 +186,39 @@ def set_tie_rule(generator):
     KS+PBS of the oracle: the RTL's (False) or the reference generator's
     (True).  keyswitch() takes its rule as an argument instead."""
     lib().or_set_tie_rule(int(bool(generator)))
+
+
+def keygen(n, N, seed, ks_bl=3, ks_lc=6, ks_w=21, pbs_bl=23):
+    """Seeded keys without the engine library: {lwe_key, glwe_key, ksk, bsk}
+    (the layouts and values of luthe_b200.keygen for the same seed)."""
+    k = {"lwe_key": np.zeros(n, np.uint32), "glwe_key": np.zeros(N, np.uint32),
+         "ksk": np.zeros((n + 1) * N * ks_lc, np.uint32), "bsk": np.zeros(n * 4 * N, np.uint64)}
+    lib().or_keygen(n, N, ks_bl, ks_lc, ks_w, pbs_bl, seed, _p(k["lwe_key"]), _p(k["glwe_key"]), _p(k["ksk"]),
+                    _p(k["bsk"]))
+    return k
+
+
+def encrypt(glwe_key, msgs, seed, bits=5):
+    msgs = np.ascontiguousarray(msgs, np.uint32)
+    N = glwe_key.size
+    out = np.zeros((msgs.size, N + 1), np.uint64)
+    lib().or_encrypt(N, bits, _p(np.ascontiguousarray(glwe_key, np.uint32)), _p(msgs), msgs.size, seed, _p(out))
+    return out
+
+
+def decrypt(glwe_key, blwe, bits=5):
+    N = glwe_key.size
+    blwe = np.ascontiguousarray(blwe, np.uint64).reshape(-1, N + 1)
+    out = np.zeros(blwe.shape[0], np.uint32)
+    lib().or_decrypt(N, bits, _p(np.ascontiguousarray(glwe_key, np.uint32)), _p(blwe), blwe.shape[0], _p(out))
+    return out
+
+
+def lut_build(N, table, bits=5):
+    table = np.ascontiguousarray(table, np.uint32)
+    out = np.zeros(2 * N, np.uint64)
+    lib().or_lut_build(N, bits, _p(table), _p(out))
+    return out
 
 
 def set_threads(t):

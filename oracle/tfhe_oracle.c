@@ -515,3 +515,136 @@ void or_set_threads(int t)
     (void)t;
 #endif
 }
+
+/* ------------------------------------------------- keys, ciphertexts, LUTs */
+
+/*
+ * Seeded key material for the CPU reference timing and the CPU tests, so that
+ * they need nothing from the engine library.  Every random word is a pure
+ * function of (seed, stream, index) through the SplitMix64 finaliser:
+ *   rnd(seed, stream, i) = mix(mix(seed ^ mix(stream * 0x100000001B3)) + i)
+ * with the stream numbers below.  With the same seed the results equal
+ * luthe_keygen / luthe_encrypt (tests/test_oracle_keygen.py checks this).
+ * Keys are binary; the KSK level z of mask coefficient y encrypts
+ * S_y 2^(W - bl (L - z)) under the LWE key mod 2^W; the BSK is a GGSW of
+ * each LWE key bit over Z_2^64 (gadget 2^(64 - pbs_bl), one level), each
+ * coefficient rounded to Z_p by or_modsw_q_to_p.
+ */
+static uint64_t kg_mix(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static uint64_t kg_rnd(uint64_t seed, uint64_t stream, uint64_t idx)
+{
+    return kg_mix(kg_mix(seed ^ kg_mix(stream * 0x100000001B3ull)) + idx);
+}
+/* Box-Muller on two uniforms, rounded to the nearest integer */
+static int64_t kg_gauss(uint64_t seed, uint64_t stream, uint64_t idx, double sigma)
+{
+    if (sigma <= 0) return 0;
+    double u1 = ((kg_rnd(seed, stream, 2 * idx) >> 11) + 1) * (1.0 / 9007199254740993.0);
+    double u2 = (kg_rnd(seed, stream, 2 * idx + 1) >> 11) * (1.0 / 9007199254740992.0);
+    double g = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+    return (int64_t)llround(g * sigma);
+}
+enum { KG_LWE_KEY = 1, KG_GLWE_KEY, KG_KSK_MASK, KG_KSK_NOISE, KG_BSK_MASK, KG_BSK_NOISE, KG_ENC_MASK, KG_ENC_NOISE };
+#define KG_LWE_SIGMA 5.3943e-6   /* 2^-17.5 of the modulus */
+#define KG_GLWE_SIGMA 4.4409e-16 /* 2^-51 of the modulus */
+
+void or_keygen(uint32_t n, uint32_t N, uint32_t ks_bl, uint32_t ks_lc, uint32_t ks_w, uint32_t pbs_bl,
+               uint64_t seed, uint32_t *lwe_key, uint32_t *glwe_key, uint32_t *ksk, uint64_t *bsk_std_p)
+{
+    for (uint32_t i = 0; i < n; i++) lwe_key[i] = kg_rnd(seed, KG_LWE_KEY, i) & 1;
+    for (uint32_t j = 0; j < N; j++) glwe_key[j] = kg_rnd(seed, KG_GLWE_KEY, j) & 1;
+    const uint32_t M = ks_w == 32 ? 0xFFFFFFFFu : ((1u << ks_w) - 1);
+    const double ks_sigma = KG_LWE_SIGMA * ldexp(1.0, (int)ks_w);
+#pragma omp parallel for schedule(static)
+    for (long yz = 0; yz < (long)N * ks_lc; yz++) {
+        const uint32_t y = (uint32_t)(yz / ks_lc), z = (uint32_t)(yz % ks_lc);
+        uint32_t body = 0;
+        for (uint32_t x = 0; x < n; x++) {
+            uint32_t a = (uint32_t)kg_rnd(seed, KG_KSK_MASK, (uint64_t)yz * n + x) & M;
+            ksk[((size_t)x * N + y) * ks_lc + z] = a;
+            body += a * lwe_key[x];
+        }
+        body += (uint32_t)kg_gauss(seed, KG_KSK_NOISE, yz, ks_sigma);
+        body += glwe_key[y] << (ks_w - ks_bl * (ks_lc - z));
+        ksk[((size_t)n * N + y) * ks_lc + z] = body & M;
+    }
+    const double glwe_sigma = KG_GLWE_SIGMA * 18446744073709551616.0;
+    const uint64_t g = 1ull << (64 - pbs_bl);
+#pragma omp parallel
+    {
+        uint64_t *A = malloc(N * 8), *B = malloc(N * 8);
+#pragma omp for schedule(dynamic, 4)
+        for (long ir = 0; ir < (long)n * 2; ir++) {
+            const uint32_t i = (uint32_t)(ir / 2), row = (uint32_t)(ir % 2);
+            for (uint32_t c = 0; c < N; c++) {
+                A[c] = kg_rnd(seed, KG_BSK_MASK, (uint64_t)ir * N + c);
+                B[c] = (uint64_t)kg_gauss(seed, KG_BSK_NOISE, (uint64_t)ir * N + c, glwe_sigma);
+            }
+            for (uint32_t j = 0; j < N; j++) /* B += A * S mod (X^N + 1, 2^64) */
+                if (glwe_key[j])
+                    for (uint32_t c = 0; c < N; c++) {
+                        uint32_t k = c + j;
+                        if (k < N) B[k] += A[c];
+                        else B[k - N] -= A[c];
+                    }
+            if (lwe_key[i]) {
+                if (row == 0) A[0] += g;
+                else B[0] += g;
+            }
+            uint64_t *dst = bsk_std_p + ((size_t)i * 2 + row) * 2 * N;
+            for (uint32_t c = 0; c < N; c++) {
+                dst[c] = or_modsw_q_to_p(A[c]);
+                dst[N + c] = or_modsw_q_to_p(B[c]);
+            }
+        }
+        free(A);
+        free(B);
+    }
+}
+
+/* BLWE encryptions (mask N coefficients, body) of msgs[c] << (64 - bits),
+ * bits = 1 + msg + carry, under the GLWE key seen as an LWE key. */
+void or_encrypt(uint32_t N, uint32_t bits, const uint32_t *S, const uint32_t *msgs, uint64_t count, uint64_t seed,
+                uint64_t *blwe)
+{
+    const double sigma = KG_GLWE_SIGMA * 18446744073709551616.0;
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < (long)count; c++) {
+        uint64_t *ct = blwe + (size_t)c * (N + 1), b = 0;
+        for (uint32_t j = 0; j < N; j++) {
+            ct[j] = kg_rnd(seed, KG_ENC_MASK, (uint64_t)c * N + j);
+            if (S[j]) b += ct[j];
+        }
+        b += (uint64_t)kg_gauss(seed, KG_ENC_NOISE, (uint64_t)c, sigma);
+        ct[N] = b + ((uint64_t)msgs[c] << (64 - bits));
+    }
+}
+
+void or_decrypt(uint32_t N, uint32_t bits, const uint32_t *S, const uint64_t *blwe, uint64_t count, uint32_t *msgs)
+{
+    for (size_t c = 0; c < count; c++) {
+        const uint64_t *ct = blwe + c * (N + 1);
+        uint64_t ph = ct[N];
+        for (uint32_t j = 0; j < N; j++)
+            if (S[j]) ph -= ct[j];
+        msgs[c] = (uint32_t)(((ph + (1ull << (63 - bits))) >> (64 - bits)) & ((1ull << bits) - 1));
+    }
+}
+
+/* Trivial LUT GLWE of table[0 .. 2^(bits-1)): box m of N / 2^(bits-1)
+ * coefficients holds f(m) << (64 - bits), rotated by half a box, the entries
+ * past X^N negated (negacyclic); the layout of the reference's LUT vectors. */
+void or_lut_build(uint32_t N, uint32_t bits, const uint32_t *table, uint64_t *glwe)
+{
+    const uint32_t nm = 1u << (bits - 1), box = N / nm, half = box / 2;
+    memset(glwe, 0, (size_t)N * 8);
+    for (uint32_t j = 0; j < N; j++)
+        glwe[N + j] = j < N - half ? (uint64_t)table[((j + half) / box) % nm] << (64 - bits)
+                                   : (uint64_t)0 - ((uint64_t)table[0] << (64 - bits));
+}
