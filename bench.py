@@ -351,13 +351,15 @@ def hbm_peak_gbs():
     return 6650.0, "fallback (earlier measurement on this pool)"
 
 
-def br_launches_per_step(B, nsm, g):
+def br_launches_per_step(B, nsm, g, tail_max=None):
     """Blind-rotation launches of one KS+PBS call (luthe_b200/csrc/kernels.cu,
-    launch_blind_rotate): one, or two when a partial last wave of at most one
-    ciphertext per SM is split off and run one ciphertext per CTA."""
+    launch_blind_rotate): one, or two when a partial last wave of at most
+    tail_max ciphertexts (default: the SM count) is split off into its own
+    launch."""
     wave = nsm * g
     tail = B % wave
-    return 2 if (g > 1 and B > wave and 0 < tail <= nsm) else 1
+    tail_max = nsm if tail_max is None or tail_max < 0 else tail_max
+    return 2 if (g > 1 and B > wave and 0 < tail <= tail_max) else 1
 
 
 def config_dict():
@@ -424,7 +426,7 @@ def main():
     eng = L.Engine(params, device=local)
     eng.upload_keys(keys)
     eng.upload_luts(luts)
-    tune = eng.autotune(592)
+    tune = eng.autotune(0)
     eng.reserve(B)
 
     d_in = torch.from_numpy(ct.view(np.int64)).cuda()
@@ -607,7 +609,8 @@ def main():
     # our kernels inside the timed region: per step one key switch and one or
     # two blind-rotation launches
     nsm = torch.cuda.get_device_properties(local).multi_processor_count
-    launches = args.steps * (1 + br_launches_per_step(B, nsm, (tune.get("chosen") or {}).get("cts_per_cta", 2)))
+    chosen = tune.get("chosen") or {}
+    launches = args.steps * (1 + br_launches_per_step(B, nsm, chosen.get("cts_per_cta", 2), chosen.get("tail_max")))
 
     if rank == 0:
         q = lambda xs, p: float(np.percentile(xs, p))
@@ -634,7 +637,7 @@ def main():
                     "d2h_bytes_per_step": int(ct.nbytes), "ms_per_step": statistics.mean(e2e_ms)},
             "gpu_launches": launches,
             "clocks": clk,
-            "autotune": tune.get("chosen"),
+            "autotune": tune,
             "serving": serve,
             "serving_150": serve_light,
             "other_configs": other,

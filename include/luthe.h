@@ -203,12 +203,28 @@ int luthe_server_step(luthe_server *srv, uint32_t *n_completed, uint32_t *n_acti
 int luthe_server_fetch(luthe_server *srv, uint64_t id, uint64_t *h_dst, double *latency_s, double *queue_s);
 int luthe_server_counters(luthe_server *srv, uint64_t *rounds, uint64_t *pbs, uint64_t *alu, uint64_t *launches);
 
-/* Blind-rotation launch shape: ciphertexts per CTA sharing one BSK slab (1 or
- * 2) and CTAs per SM of the persistent grid.  luthe_autotune times the
- * candidates on `sample` ciphertexts and keeps the fastest; it writes a JSON
- * record of the trial into `json` (may be NULL). */
+/* Blind-rotation launch shape (the HPU's batch configuration: the BSK slice
+ * shared per batch, hw/module/pe_pbs/module/pep_sequencer/rtl/
+ * pep_sequencer.sv:573-620, docs/hpu_parameters.md): ciphertexts per CTA
+ * sharing one BSK slab (1 or 2) and CTAs per SM of the persistent grid;
+ * luthe_set_br_config resets the batch-size cut-offs below to their defaults.
+ *
+ * luthe_autotune times, on this device, (1) one and two ciphertexts per CTA
+ * on `sample` ciphertexts (0: four waves), (2) for batches of 1/8 .. 3/2 of
+ * the SM count, one ciphertext per 2-SM cluster, one per CTA, and the
+ * two-per-CTA launch, and (3) for partial last waves of 1/4 .. 7/4 of the SM
+ * count, a separate small launch against one launch for all; it keeps the
+ * fastest shape and cut-offs and writes a JSON record of every trial and the
+ * choice into `json` (may be NULL).  When the environment variable
+ * LUTHE_TUNING_DIR names a directory, the choice is also saved there, one
+ * file per device and parameter set, and luthe_ctx_create loads that file if
+ * it exists.  luthe_tuning_save / luthe_tuning_load write and read the choice
+ * at an explicit path; loading refuses a file made for another device model,
+ * SM count or parameter set. */
 int luthe_set_br_config(luthe_ctx *ctx, int cts_per_cta, int ctas_per_sm);
 int luthe_autotune(luthe_ctx *ctx, size_t sample, char *json, size_t json_cap);
+int luthe_tuning_save(luthe_ctx *ctx, const char *path);
+int luthe_tuning_load(luthe_ctx *ctx, const char *path);
 
 /* Device-side error flags raised by blind rotations since the last check
  * (sticky, cleared by this call; the stream must have been synchronised):

@@ -35,6 +35,7 @@ SYMBOLS = [
     "luthe_server_create", "luthe_server_destroy", "luthe_server_submit", "luthe_server_step",
     "luthe_server_fetch", "luthe_server_counters", "luthe_blind_rotate", "luthe_ntt_fwd",
     "luthe_ntt_inv", "luthe_ntt_mul", "luthe_lwe_op", "luthe_set_br_config", "luthe_autotune",
+    "luthe_tuning_save", "luthe_tuning_load",
     "luthe_check_device_error", "luthe_measure_int_peak", "luthe_keygen", "luthe_encrypt", "luthe_decrypt", "luthe_lut_build",
 ]
 
@@ -100,6 +101,8 @@ def lib():
         L.luthe_lwe_op.argtypes = [vp, ctypes.c_int, vp, vp, vp, u64, sz, vp]
         L.luthe_set_br_config.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.luthe_autotune.argtypes = [vp, sz, ctypes.c_char_p, sz]
+        L.luthe_tuning_save.argtypes = [vp, ctypes.c_char_p]
+        L.luthe_tuning_load.argtypes = [vp, ctypes.c_char_p]
         L.luthe_check_device_error.argtypes = [vp]
         L.luthe_measure_int_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double)]
@@ -323,9 +326,17 @@ class Engine:
         _check(lib().luthe_set_br_config(self._h, cts_per_cta, ctas_per_sm))
 
     def autotune(self, sample=0):
-        buf = ctypes.create_string_buffer(4096)
-        _check(lib().luthe_autotune(self._h, sample, buf, 4096))
+        """Time the blind rotation's launch forms on this device and keep the
+        fastest (luthe_autotune); returns the record of trials and the choice."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        _check(lib().luthe_autotune(self._h, sample, buf, 1 << 16))
         return json.loads(buf.value.decode())
+
+    def tuning_save(self, path):
+        _check(lib().luthe_tuning_save(self._h, str(path).encode()))
+
+    def tuning_load(self, path):
+        _check(lib().luthe_tuning_load(self._h, str(path).encode()))
 
     def check_device_error(self):
         _check(lib().luthe_check_device_error(self._h))

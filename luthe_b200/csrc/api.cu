@@ -5,7 +5,9 @@
 #include <stdlib.h>
 #include <string.h>
 #include <stdarg.h>
+#include <algorithm>
 #include <atomic>
+#include <ctype.h>
 #include <string>
 #include <vector>
 #include "../../include/luthe.h"
@@ -77,6 +79,8 @@ void drop_graphs(luthe_ctx *c)
     c->graphs.clear();
 }
 
+int tuning_autoload(luthe_ctx *c);
+
 extern "C" int luthe_ctx_create(const luthe_params *p, int device, uint64_t budget, luthe_ctx **out)
 {
     if (!out) return fail(LUTHE_E_PARAM, "null out");
@@ -111,6 +115,10 @@ extern "C" int luthe_ctx_create(const luthe_params *p, int device, uint64_t budg
     if (e != cudaSuccess) {
         luthe_ctx_destroy(c);
         return fail(LUTHE_E_CUDA, "context init: %s", cudaGetErrorString(e));
+    }
+    if ((r = tuning_autoload(c))) {
+        luthe_ctx_destroy(c);
+        return r;
     }
     *out = c;
     return LUTHE_OK;
@@ -464,23 +472,167 @@ extern "C" int luthe_check_device_error(luthe_ctx *c)
     return LUTHE_OK;
 }
 
+// ------------------------------------------------------------ autotuner
+//
+// The blind rotation's launch shape is chosen per batch size (kernels.cu,
+// launch_blind_rotate): ciphertexts per CTA (G), and the batch sizes up to
+// which a batch runs one ciphertext per 2-SM cluster (pair_max) or one per
+// CTA (split_max), and up to which a partial last wave runs as its own launch
+// of those forms (tail_max).  The autotuner times every form around each
+// decision point on this device and keeps the fastest; the choice can be
+// saved as JSON and loaded by later contexts (the counterpart of the HPU's
+// batch configuration, pep_sequencer.sv:573-620 and docs/hpu_parameters.md).
+
+namespace {
+
+struct Timer {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    Timer() { cudaEventCreate(&e0); cudaEventCreate(&e1); }
+    ~Timer() { cudaEventDestroy(e0); cudaEventDestroy(e1); }
+};
+
+// median of three timed launches after one untimed launch, in ms; < 0 on error
+float time_br(luthe_ctx *c, const BrConfig &cfg, const uint32_t *d_l, const uint32_t *d_ids, uint64_t *d_o, size_t B,
+              Timer &t)
+{
+    const uint32_t n = c->p.lwe_dim;
+    float ms[3];
+    for (int r = -1; r < 3; r++) {
+        if (r >= 0) cudaEventRecord(t.e0, 0);
+        cudaError_t e = launch_blind_rotate(cfg, c->nsm, d_l, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_o, B, n,
+                                            c->d_err, 0, nullptr, 1, c->p.pbs_base_log, c->tie_rule);
+        if (e != cudaSuccess) return -1.f;
+        if (r >= 0) {
+            cudaEventRecord(t.e1, 0);
+            if (cudaEventSynchronize(t.e1) != cudaSuccess) return -1.f;
+            cudaEventElapsedTime(&ms[r], t.e0, t.e1);
+        }
+    }
+    if (ms[0] > ms[1]) std::swap(ms[0], ms[1]);
+    if (ms[1] > ms[2]) std::swap(ms[1], ms[2]);
+    if (ms[0] > ms[1]) std::swap(ms[0], ms[1]);
+    return ms[1];
+}
+
+std::string tuning_key(const luthe_ctx *c)
+{
+    cudaDeviceProp prop;
+    std::string name = cudaGetDeviceProperties(&prop, c->device) == cudaSuccess ? prop.name : "unknown";
+    for (auto &ch : name)
+        if (!isalnum((unsigned char)ch)) ch = '_';
+    char buf[160];
+    snprintf(buf, sizeof buf, "%s_sm%d_n%u_ks%ux%u_pbs%u", name.c_str(), c->nsm, c->p.lwe_dim, c->p.ks_base_log,
+             c->p.ks_level, c->p.pbs_base_log);
+    return buf;
+}
+
+std::string tuning_json(const luthe_ctx *c)
+{
+    char buf[512];
+    snprintf(buf, sizeof buf,
+             "{\"format\":\"luthe-tuning-1\",\"key\":\"%s\",\"cts_per_cta\":%d,\"ctas_per_sm\":%d,"
+             "\"pair_max\":%d,\"split_max\":%d,\"tail_max\":%d}",
+             tuning_key(c).c_str(), c->br.cts_per_cta, c->br.ctas_per_sm, c->br.pair_max, c->br.split_max,
+             c->br.tail_max);
+    return buf;
+}
+
+// integer value of "key": in a flat JSON object written by tuning_json
+bool json_int(const std::string &js, const char *key, int *out)
+{
+    const std::string k = std::string("\"") + key + "\":";
+    size_t at = js.find(k);
+    if (at == std::string::npos) return false;
+    char *end = nullptr;
+    long v = strtol(js.c_str() + at + k.size(), &end, 10);
+    if (end == js.c_str() + at + k.size()) return false;
+    *out = (int)v;
+    return true;
+}
+
+std::string tuning_dir_path(const luthe_ctx *c)
+{
+    const char *dir = getenv("LUTHE_TUNING_DIR");
+    if (!dir || !*dir) return "";
+    return std::string(dir) + "/luthe_tune_" + tuning_key(c) + ".json";
+}
+
+}  // namespace
+
+extern "C" int luthe_tuning_load(luthe_ctx *c, const char *path)
+{
+    if (!c || !path) return fail(LUTHE_E_PARAM, "null argument");
+    FILE *f = fopen(path, "r");
+    if (!f) return fail(LUTHE_E_PARAM, "tuning file %s: cannot open", path);
+    std::string js;
+    char buf[1024];
+    size_t got;
+    while ((got = fread(buf, 1, sizeof buf, f)) > 0) js.append(buf, got);
+    fclose(f);
+    if (js.find("\"format\":\"luthe-tuning-1\"") == std::string::npos)
+        return fail(LUTHE_E_PARAM, "tuning file %s: not a luthe-tuning-1 record", path);
+    const std::string key = "\"key\":\"" + tuning_key(c) + "\"";
+    if (js.find(key) == std::string::npos)
+        return fail(LUTHE_E_PARAM, "tuning file %s was made for another device or parameter set (want %s)", path,
+                    tuning_key(c).c_str());
+    BrConfig b = c->br;
+    if (!json_int(js, "cts_per_cta", &b.cts_per_cta) || !json_int(js, "ctas_per_sm", &b.ctas_per_sm) ||
+        !json_int(js, "pair_max", &b.pair_max) || !json_int(js, "split_max", &b.split_max) ||
+        !json_int(js, "tail_max", &b.tail_max))
+        return fail(LUTHE_E_PARAM, "tuning file %s: missing fields", path);
+    if (b.cts_per_cta < 1 || b.cts_per_cta > 2 || b.ctas_per_sm != 1)
+        return fail(LUTHE_E_PARAM, "tuning file %s: unsupported launch shape %d/%d", path, b.cts_per_cta, b.ctas_per_sm);
+    CUDA_TRY(cudaSetDevice(c->device));
+    drop_graphs(c);
+    c->br = b;
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_tuning_save(luthe_ctx *c, const char *path)
+{
+    if (!c || !path) return fail(LUTHE_E_PARAM, "null argument");
+    FILE *f = fopen(path, "w");
+    if (!f) return fail(LUTHE_E_PARAM, "tuning file %s: cannot write", path);
+    const std::string js = tuning_json(c) + "\n";
+    const bool ok = fwrite(js.data(), 1, js.size(), f) == js.size();
+    if (fclose(f) != 0 || !ok) return fail(LUTHE_E_PARAM, "tuning file %s: write failed", path);
+    return LUTHE_OK;
+}
+
+int tuning_autoload(luthe_ctx *c)
+{
+    const std::string path = tuning_dir_path(c);
+    if (path.empty()) return LUTHE_OK;
+    FILE *f = fopen(path.c_str(), "r");
+    if (!f) return LUTHE_OK;  // nothing tuned yet for this device and parameter set
+    fclose(f);
+    return luthe_tuning_load(c, path.c_str());
+}
+
 extern "C" int luthe_autotune(luthe_ctx *c, size_t sample, char *json, size_t cap)
 {
     int r = need_keys(c);
     if (r) return r;
-    if (sample == 0) sample = (size_t)c->nsm * 4;
     CUDA_TRY(cudaSetDevice(c->device));
+    const int nsm = c->nsm;
+    if (sample == 0) sample = (size_t)nsm * 8;  // four two-per-CTA waves
+    const size_t maxB = std::max(sample, (size_t)nsm * 2 + (size_t)nsm * 3 / 2);
     const uint32_t n = c->p.lwe_dim;
     uint32_t *d_l = nullptr, *d_ids = nullptr;
     uint64_t *d_o = nullptr;
-    if ((r = dalloc(c, (void **)&d_l, sample * (n + 1) * 4))) return r;
-    if ((r = dalloc(c, (void **)&d_ids, sample * 4)) || (r = dalloc(c, (void **)&d_o, sample * (N + 1) * 8))) {
-        dfree(c, d_l, sample * (n + 1) * 4);
-        dfree(c, d_ids, sample * 4);
+    if ((r = dalloc(c, (void **)&d_l, maxB * (n + 1) * 4))) return r;
+    if ((r = dalloc(c, (void **)&d_ids, maxB * 4)) || (r = dalloc(c, (void **)&d_o, maxB * (N + 1) * 8))) {
+        dfree(c, d_l, maxB * (n + 1) * 4);
+        dfree(c, d_ids, maxB * 4);
         return r;
     }
+    auto release = [&]() {
+        dfree(c, d_l, maxB * (n + 1) * 4);
+        dfree(c, d_ids, maxB * 4);
+        dfree(c, d_o, maxB * (N + 1) * 8);
+    };
     // deterministic pseudo-random mod-switched inputs
-    std::vector<uint32_t> hl(sample * (n + 1));
+    std::vector<uint32_t> hl(maxB * (n + 1));
     uint64_t st = 0x9E3779B97F4A7C15ull;
     for (auto &v : hl) {
         st ^= st << 13;
@@ -488,61 +640,66 @@ extern "C" int luthe_autotune(luthe_ctx *c, size_t sample, char *json, size_t ca
         st ^= st << 17;
         v = (uint32_t)(st & (TWO_N - 1));
     }
-    cudaMemcpy(d_l, hl.data(), hl.size() * 4, cudaMemcpyHostToDevice);
-    cudaMemset(d_ids, 0, sample * 4);
-    const BrConfig cands[] = {{1, 1}, {2, 1}};
+    cudaError_t ce = cudaMemcpy(d_l, hl.data(), hl.size() * 4, cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaMemset(d_ids, 0, maxB * 4);
+    if (ce != cudaSuccess) {
+        release();
+        return fail(LUTHE_E_CUDA, "autotune: %s", cudaGetErrorString(ce));
+    }
+    Timer tm;
     std::string rec = "{\"sample\":" + std::to_string(sample) + ",\"trials\":[";
-    float best = 1e30f;
-    BrConfig best_cfg = c->br;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    bool first = true;
-    for (const BrConfig &cfg : cands) {
-        size_t smem = br_smem_bytes(cfg, n);
-        int max_smem = 0;
-        cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
-        if ((size_t)max_smem < cfg.ctas_per_sm * (smem + 1024)) continue;
-        cudaError_t e = launch_blind_rotate(cfg, c->nsm, d_l, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_o,
-                                            sample, n, c->d_err, 0, nullptr, 1, c->p.pbs_base_log, c->tie_rule);
-        cudaEventRecord(e0, 0);
-        for (int rep = 0; rep < 2 && e == cudaSuccess; rep++)
-            e = launch_blind_rotate(cfg, c->nsm, d_l, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_o, sample, n,
-                                    c->d_err, 0, nullptr, 1, c->p.pbs_base_log, c->tie_rule);
-        cudaEventRecord(e1, 0);
-        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-        if (e != cudaSuccess) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            dfree(c, d_l, sample * (n + 1) * 4);
-            dfree(c, d_ids, sample * 4);
-            dfree(c, d_o, sample * (N + 1) * 8);
-            return fail(LUTHE_E_CUDA, "autotune: %s", cudaGetErrorString(e));
-        }
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        ms /= 2;
-        char buf[160];
-        snprintf(buf, sizeof buf, "%s{\"cts_per_cta\":%d,\"ctas_per_sm\":%d,\"ms\":%.4f,\"bootstraps_per_s\":%.1f}",
-                 first ? "" : ",", cfg.cts_per_cta, cfg.ctas_per_sm, ms, sample / (ms * 1e-3));
+    bool first = true, failed = false;
+    auto trial = [&](const char *what, size_t B, const BrConfig &cfg) -> float {
+        float ms = time_br(c, cfg, d_l, d_ids, d_o, B, tm);
+        if (ms < 0) failed = true;
+        char buf[200];
+        snprintf(buf, sizeof buf, "%s{\"form\":\"%s\",\"B\":%zu,\"ms\":%.4f}", first ? "" : ",", what, B, ms);
         rec += buf;
         first = false;
-        if (ms < best) {
-            best = ms;
-            best_cfg = cfg;
-        }
+        return ms;
+    };
+    const int BIG = 1 << 30;
+    BrConfig best = c->br;
+    // 1. ciphertexts per CTA on full waves
+    {
+        BrConfig g1{1, 1, 0, 0, 0}, g2{2, 1, 0, 0, 0};
+        const float t1 = trial("G1", sample, g1), t2 = trial("G2", sample, g2);
+        best.cts_per_cta = (t1 >= 0 && t1 < t2) ? 1 : 2;
+        best.ctas_per_sm = 1;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    dfree(c, d_l, sample * (n + 1) * 4);
-    dfree(c, d_ids, sample * 4);
-    dfree(c, d_o, sample * (N + 1) * 8);
+    if (best.cts_per_cta == 2 && !failed) {
+        // 2. small batches: 2-SM clusters, one per CTA, or a two-per-CTA launch
+        int pair_max = 0, split_max = 0;
+        for (int k = 1; k <= 12; k++) {
+            const size_t B = (size_t)nsm * k / 8;
+            if (B == 0) continue;
+            const float tp = trial("pair", B, BrConfig{2, 1, BIG, BIG, 0});
+            const float ts = trial("split", B, BrConfig{2, 1, 0, BIG, 0});
+            const float tw = trial("wave", B, BrConfig{2, 1, 0, 0, 0});
+            if (tp >= 0 && tp <= ts && tp <= tw) pair_max = (int)B;
+            if (std::min(tp, ts) >= 0 && std::min(tp, ts) < tw) split_max = (int)B;
+        }
+        // 3. a partial last wave: its own small launch, or part of the wave launch
+        int tail_max = 0;
+        for (int k = 1; k <= 8; k++) {
+            const size_t t = (size_t)nsm * k / 4, B = (size_t)2 * nsm + t;
+            if (t == 0 || t >= (size_t)2 * nsm || B > maxB) continue;
+            const float ta = trial("wave+tail", B, BrConfig{2, 1, pair_max, split_max, BIG});
+            const float tb = trial("waves", B, BrConfig{2, 1, pair_max, split_max, 0});
+            if (ta >= 0 && ta < tb) tail_max = (int)t;
+        }
+        best.pair_max = pair_max;
+        best.split_max = std::max(split_max, pair_max);
+        best.tail_max = tail_max;
+    }
+    release();
+    if (failed) return fail(LUTHE_E_CUDA, "autotune: a trial launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     drop_graphs(c);
-    c->br = best_cfg;
-    char tail[96];
-    snprintf(tail, sizeof tail, "],\"chosen\":{\"cts_per_cta\":%d,\"ctas_per_sm\":%d}}", best_cfg.cts_per_cta,
-             best_cfg.ctas_per_sm);
-    rec += tail;
+    c->br = best;
+    rec += "],\"chosen\":" + tuning_json(c);
+    const std::string path = tuning_dir_path(c);
+    if (!path.empty() && (r = luthe_tuning_save(c, path.c_str()))) return r;
+    rec += ",\"saved_to\":\"" + path + "\"}";
     if (json && cap) {
         strncpy(json, rec.c_str(), cap - 1);
         json[cap - 1] = 0;

@@ -1081,18 +1081,22 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
     if (tie_rule != TIE_RTL && tie_rule != TIE_GENERATOR) return cudaErrorInvalidValue;
     const int G = cfg.cts_per_cta, cps = cfg.ctas_per_sm;
     const size_t wave = (size_t)nsm * cps * G;
+    const size_t pair_max = cfg.pair_max >= 0 ? (size_t)cfg.pair_max : (size_t)(nsm / 2);
+    const size_t split_max = cfg.split_max >= 0 ? (size_t)cfg.split_max : (size_t)nsm;
+    const size_t tail_max = cfg.tail_max >= 0 ? (size_t)cfg.tail_max : (size_t)nsm;
     // A batch that fits one ciphertext per SM runs in the latency form (one
     // ciphertext per CTA, its polynomials split over the two groups): with
     // G = 2 ciphertexts per CTA half the SMs would idle.
     // At most one ciphertext per two SMs: the two-SM form, lower latency still.
-    auto small_form = [&](size_t count) { return count <= (size_t)(nsm / 2) ? -1 : 0; };
-    if (G > 1 && B <= (size_t)nsm)
+    // (Both forms are persistent over their ciphertexts, so any cut-off is correct.)
+    auto small_form = [&](size_t count) { return count <= pair_max ? -1 : 0; };
+    if (G > 1 && B <= split_max)
         return launch_br_once(small_form(B), 1, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, B, n,
                               d_err, s, d_dst_idx, mlk, pbs_bw, tie_rule);
     // A partial last wave of at most one ciphertext per SM runs as its own
     // latency-form launch after the full waves instead of a full G-per-CTA wave.
     const size_t tail = B % wave;
-    if (G > 1 && B > wave && tail > 0 && tail <= (size_t)nsm) {
+    if (G > 1 && B > wave && tail > 0 && tail <= tail_max) {
         const size_t full = B - tail;
         cudaError_t e = launch_br_once(G, cps, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, full, n,
                                        d_err, s, d_dst_idx, mlk, pbs_bw, tie_rule);

@@ -20,6 +20,11 @@ constexpr size_t SLAB_BYTES = SLAB_WORDS * 8; // 64 KiB
 struct BrConfig {
     int cts_per_cta;    // ciphertexts sharing one BSK slab per CTA (G)
     int ctas_per_sm;    // resident CTAs per SM of the persistent grid
+    // batch-size cut-offs of the launch forms (launch_blind_rotate); -1 keeps
+    // the default named beside each.  The autotuner (luthe_autotune) sets them.
+    int pair_max = -1;   // batches up to this run one ciphertext per 2-SM cluster (default SMs / 2)
+    int split_max = -1;  // ... else up to this, one ciphertext per CTA (default SMs)
+    int tail_max = -1;   // a partial last wave up to this runs as its own small launch (default SMs)
 };
 
 // device twiddle tables: [fwd 8x256][inv 8x256]
