@@ -32,11 +32,12 @@ def test_autotune_choice_is_saved_loaded_and_exact(engine, params, keys, oracle_
     d = tmp_path / "dir"
     d.mkdir()
     (d / f"luthe_tune_{chosen['key']}.json").write_text(path.read_text())
-    code = ("import luthe_b200 as L, json; e = L.Engine(); print(json.dumps(e.autotune_state()))"
-            if hasattr(L.Engine, "autotune_state") else "import luthe_b200 as L; L.Engine(); print('ok')")
+    seen = tmp_path / "seen.json"
+    code = "import sys, luthe_b200 as L; L.Engine().tuning_save(sys.argv[1])"
     env = dict(os.environ, LUTHE_TUNING_DIR=str(d))
-    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True)
+    out = subprocess.run([sys.executable, "-c", code, str(seen)], cwd=ROOT, env=env, capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
+    assert json.loads(seen.read_text()) == chosen
     # a file for another device or parameter set is refused
     bad = tmp_path / "bad.json"
     bad.write_text(path.read_text().replace(chosen["key"], "other_device"))
