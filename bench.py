@@ -198,10 +198,12 @@ def max_over_ranks(x, dist, device):
     return float(t.item())
 
 
-def serving(L, eng, params, keys, seed, n_req=400, rate=300.0):
+def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_per_kind=8):
     """Serving loop under Poisson arrivals of 16-bit radix IOps (50 % ADD with
     carry propagation, 30 % scalar compare, 20 % multiply); every result is
-    checked by decryption."""
+    checked by decryption, and with `ob` (an oracle BSK) the first
+    `check_per_kind` requests of each kind bit for bit against the oracle's
+    run of the same DOp programs (not timed)."""
     from luthe_b200 import iops as I
     eng.upload_luts(np.stack([L.lut_build(params, t) for t in I.lut_tables()]))
     rng = np.random.default_rng(seed)
@@ -255,7 +257,16 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0):
         dec = [int(x) for x in L.decrypt(params, keys["glwe_key"], outs[r])]
         ok += (I.from_blocks(dec) if reqs[r][2] == 8 else dec[0]) == expect[r]
     ls = np.array([lat[r] for r in range(n_req)]) * 1e3
+    exact = None
+    if ob is not None:
+        from oracle import dops
+        sel = [r for kind in range(3) for r in np.nonzero(kinds == kind)[0][:check_per_kind]]
+        luts = np.stack([L.lut_build(params, t) for t in I.lut_tables()])
+        want = dops.run_many([tuple(reqs[r]) for r in sel], keys["ksk"], ob, luts)
+        eq = sum(bool(np.array_equal(outs[r], w)) for r, w in zip(sel, want))
+        exact = f"{eq}/{len(sel)} (first {check_per_kind} requests of each kind, MUL included)"
     return {"requests": n_req, "arrival_rate_per_s": rate, "mix": "50% add, 30% scalar cmp, 20% mul (16-bit radix)",
+            "bit_exact_vs_oracle": exact,
             "throughput_requests_per_s": n_req / wall, "pbs_per_s": cnt["pbs"] / wall,
             "latency_ms_p50": float(np.percentile(ls, 50)), "latency_ms_p99": float(np.percentile(ls, 99)),
             "rounds": cnt["rounds"], "pbs": cnt["pbs"], "alu_dops": cnt["alu"], "launches": cnt["launches"],
@@ -468,6 +479,7 @@ def main():
         evs.append((e0, e1))
     torch.cuda.synchronize()
     clk = clocks.stop()
+    step_out = d_out.cpu().numpy().view(np.uint64).copy()  # the timed step's outputs, checked at the end
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = max_over_ranks(sum(step_ms), dist, "cuda")
     if dist:
@@ -587,7 +599,9 @@ def main():
     # grows) and at 150 req/s (inside it)
     serve = serve_light = None
     if world == 1 and not args.no_serving:
-        serve = serving(L, eng, params, keys, args.seed + 99)
+        import oracle
+        serve_ob = oracle.OracleBsk(keys["bsk"], params.lwe_dim, params.poly_size) if args.cpu_sample > 0 else None
+        serve = serving(L, eng, params, keys, args.seed + 99, ob=serve_ob)
         serve_light = serving(L, eng, params, keys, args.seed + 98, rate=150.0)
 
     # ---- CPU baseline (rank 0, one GPU): the CPU restatement on all host cores
@@ -601,10 +615,15 @@ def main():
         t0 = time.perf_counter()
         out = ob.ks_pbs(keys["ksk"], ct[:s], luts, ids[:s])
         dt = time.perf_counter() - t0
-        gpu_first = d_out[:s].cpu().numpy().view(np.uint64)
         cpu = {"value": s / dt, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"first {s} BLWEs of the workload, KS+PBS, {dt:.1f} s",
-               "bit_exact_vs_gpu": bool(np.array_equal(out, gpu_first))}
+               "bit_exact_vs_gpu": bool(np.array_equal(out, step_out[:s]))}
+        # every output of the timed step against the oracle (not timed)
+        t0 = time.perf_counter()
+        want = ob.ks_pbs(keys["ksk"], ct, luts, ids)
+        eq = int((want == step_out).all(axis=1).sum())
+        cpu["bit_exact_all"] = f"{eq}/{B}"
+        cpu["bit_exact_all_s"] = round(time.perf_counter() - t0, 1)
 
     # our kernels inside the timed region: per step one key switch and one or
     # two blind-rotation launches

@@ -54,60 +54,27 @@ def test_many_lut_matches_oracle(engine, params, keys, oracle_bsk, mlk, count):
 
 
 def oracle_run(program, src, n_dst, keys, oracle_bsk, luts):
-    """Execute a DOp program on ciphertexts with the CPU oracle (PBS runs of
-    mutually independent PBS DOps are batched)."""
-    regs = {}
-    dst = [None] * n_dst
-    words = [int(w) for w in program]
-    i = 0
-    while i < len(words):
-        w = words[i]
-        op, d, s0, s1 = w >> 26, w & 0x7F, (w >> 7) & 0x7F, (w >> 14) & 0x7F
-        if op >= 0x30:
-            batch, written = [], set()
-            while i < len(words) and (words[i] >> 26) >= 0x30 and ((words[i] >> 7) & 0x7F) not in written:
-                ww = words[i]
-                k = 1 << ((ww >> 26) - 0x30)
-                batch.append(ww)
-                written.update(range(ww & 0x7F, (ww & 0x7F) + k))
-                i += 1
-            ks = sorted({1 << ((x >> 26) - 0x30) for x in batch})
-            for k in ks:
-                sub = [x for x in batch if (1 << ((x >> 26) - 0x30)) == k]
-                cts = np.stack([regs[(x >> 7) & 0x7F] for x in sub])
-                gids = np.array([(x >> 14) & 0xFFF for x in sub], np.uint32)
-                out = oracle_bsk.ks_pbs(keys["ksk"], cts, luts, gids, mlk=k)
-                for j, x in enumerate(sub):
-                    for m in range(k):
-                        regs[(x & 0x7F) + m] = out[j * k + m]
-            continue
-        with np.errstate(over="ignore"):
-            if op == 0x20:
-                regs[d] = src[(w >> 10) & 0xFFFF].copy()
-            elif op == 0x21:
-                dst[(w >> 10) & 0xFFFF] = regs[d].copy()
-            elif op == 0x01:
-                regs[d] = regs[s0] + regs[s1]
-            elif op == 0x05:
-                regs[d] = regs[s0] * np.uint64((w >> 21) & 0x1F) + regs[s1]
-            else:
-                raise ValueError(hex(op))
-        i += 1
-    return np.stack(dst)
+    """Execute a DOp program on ciphertexts with the CPU oracle."""
+    from oracle import dops
+    return dops.run(program, src, n_dst, keys["ksk"], oracle_bsk, luts)
 
 
-def test_serving_add_and_cmp_bit_exact_vs_oracle(engine, params, keys, oracle_bsk, iop_luts):
+def test_serving_add_cmp_mul_bit_exact_vs_oracle(engine, params, keys, oracle_bsk, iop_luts):
     engine.upload_luts(iop_luts)
     srv = L.Server(engine, pool_bytes=256 << 20)
     a, b, k = 0xBEEF, 0x1357, 0x4000
     reqs = [(I.prog_add(), enc_blocks(params, keys, [a, b], 11), 8),
-            (I.prog_cmp_gt(k), enc_blocks(params, keys, [a], 12), 1)]
+            (I.prog_cmp_gt(k), enc_blocks(params, keys, [a], 12), 1),
+            (I.prog_mul(), enc_blocks(params, keys, [a, b], 13), 8)]
     outs = srv.run(reqs)
     srv.close()
     assert I.from_blocks(dec_blocks(params, keys, outs[0])) == (a + b) % 65536
     assert dec_blocks(params, keys, outs[1]) == [int(a > k)]
-    for (prog, src, nd), got in zip(reqs, outs):
-        assert np.array_equal(got, oracle_run(prog, src, nd, keys, oracle_bsk, iop_luts))
+    assert I.from_blocks(dec_blocks(params, keys, outs[2])) == (a * b) % 65536
+    from oracle import dops
+    want = dops.run_many(reqs, keys["ksk"], oracle_bsk, iop_luts)  # all three programs side by side
+    for got, w in zip(outs, want):
+        assert np.array_equal(got, w)
 
 
 def test_serving_mix_equals_alone(engine, params, keys, iop_luts):
