@@ -198,7 +198,7 @@ def max_over_ranks(x, dist, device):
     return float(t.item())
 
 
-def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_per_kind=8):
+def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_per_kind=8, window_us=0, fill=0):
     """Serving loop under Poisson arrivals of 16-bit radix IOps (50 % ADD with
     carry propagation, 30 % scalar compare, 20 % multiply); every result is
     checked by decryption, and with `ob` (an oracle BSK) the first
@@ -230,6 +230,7 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
     for r in reqs:
         r[1], off = ct[off:off + r[1]], off + r[1]
     srv = L.Server(eng, pool_bytes=4 << 30, max_pbs=4096)
+    srv.set_batching(fill, window_us)
     srv.run([tuple(reqs[0]), tuple(reqs[1])])          # warm-up
     base = srv.counters()
     ids, outs, lat = [None] * n_req, {}, {}
@@ -266,6 +267,7 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
         eq = sum(bool(np.array_equal(outs[r], w)) for r, w in zip(sel, want))
         exact = f"{eq}/{len(sel)} (first {check_per_kind} requests of each kind, MUL included)"
     return {"requests": n_req, "arrival_rate_per_s": rate, "mix": "50% add, 30% scalar cmp, 20% mul (16-bit radix)",
+            "batching_window_us": window_us, "batching_fill": fill or "one wave (2 per SM)",
             "bit_exact_vs_oracle": exact,
             "throughput_requests_per_s": n_req / wall, "pbs_per_s": cnt["pbs"] / wall,
             "latency_ms_p50": float(np.percentile(ls, 50)), "latency_ms_p99": float(np.percentile(ls, 99)),
@@ -597,12 +599,16 @@ def main():
     # ---- serving loop (one GPU): Poisson arrivals of radix IOps
     # at 300 req/s offered (above the loop's capacity for this mix: the queue
     # grows) and at 150 req/s (inside it)
-    serve = serve_light = None
+    serve = serve_light = serve_win = serve_light_win = None
     if world == 1 and not args.no_serving:
         import oracle
         serve_ob = oracle.OracleBsk(keys["bsk"], params.lwe_dim, params.poly_size) if args.cpu_sample > 0 else None
         serve = serving(L, eng, params, keys, args.seed + 99, ob=serve_ob)
         serve_light = serving(L, eng, params, keys, args.seed + 98, rate=150.0)
+        # the same loads with a batching window: partial PBS batches wait up
+        # to 3 ms for more work while another batch is on the GPU
+        serve_win = serving(L, eng, params, keys, args.seed + 99, window_us=3000)
+        serve_light_win = serving(L, eng, params, keys, args.seed + 98, rate=150.0, window_us=3000)
 
     # ---- CPU baseline (rank 0, one GPU): the CPU restatement on all host cores
     cpu = None
@@ -659,6 +665,8 @@ def main():
             "autotune": tune,
             "serving": serve,
             "serving_150": serve_light,
+            "serving_window_3ms": serve_win,
+            "serving_150_window_3ms": serve_light_win,
             "other_configs": other,
             "param_sets": psets,
         }

@@ -202,6 +202,14 @@ int luthe_server_step(luthe_server *srv, uint32_t *n_completed, uint32_t *n_acti
  * while it is not finished. */
 int luthe_server_fetch(luthe_server *srv, uint64_t id, uint64_t *h_dst, double *latency_s, double *queue_s);
 int luthe_server_counters(luthe_server *srv, uint64_t *rounds, uint64_t *pbs, uint64_t *alu, uint64_t *launches);
+/* Batching window of the PBS lanes, after the HPU's batch policy (a batch
+ * leaves when full or when the batch-in-progress timeout runs out,
+ * hw/module/pe_pbs/module/pep_sequencer/rtl/pep_sequencer.sv:573-620): ready
+ * PBS DOps are held back while some lane is busy, fewer than `fill` (0: two
+ * per SM, one full wave) are ready and the oldest has waited less than
+ * `window_us`.  window_us = 0 (the default) issues whatever is ready on any
+ * idle lane. */
+int luthe_server_set_batching(luthe_server *srv, uint32_t fill, uint32_t window_us);
 
 /* Blind-rotation launch shape (the HPU's batch configuration: the BSK slice
  * shared per batch, hw/module/pe_pbs/module/pep_sequencer/rtl/

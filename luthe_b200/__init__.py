@@ -33,7 +33,7 @@ SYMBOLS = [
     "luthe_upload_bsk", "luthe_upload_bsk_eval", "luthe_set_tie_rule", "luthe_upload_ksk", "luthe_upload_luts", "luthe_reserve", "luthe_ks_pbs",
     "luthe_ks_pbs_host", "luthe_ks_pbs_graph", "luthe_ks_pbs_noalloc", "luthe_ks_pbs_ml", "luthe_keyswitch",
     "luthe_server_create", "luthe_server_destroy", "luthe_server_submit", "luthe_server_step",
-    "luthe_server_fetch", "luthe_server_counters", "luthe_blind_rotate", "luthe_ntt_fwd",
+    "luthe_server_fetch", "luthe_server_counters", "luthe_server_set_batching", "luthe_blind_rotate", "luthe_ntt_fwd",
     "luthe_ntt_inv", "luthe_ntt_mul", "luthe_lwe_op", "luthe_set_br_config", "luthe_autotune",
     "luthe_tuning_save", "luthe_tuning_load",
     "luthe_check_device_error", "luthe_measure_int_peak", "luthe_keygen", "luthe_encrypt", "luthe_decrypt", "luthe_lut_build",
@@ -93,6 +93,7 @@ def lib():
         L.luthe_server_step.argtypes = [vp, pu32, pu32, pu32]
         L.luthe_server_fetch.argtypes = [vp, u64, vp, pd, pd]
         L.luthe_server_counters.argtypes = [vp, pu64, pu64, pu64, pu64]
+        L.luthe_server_set_batching.argtypes = [vp, u32, u32]
         L.luthe_keyswitch.argtypes = [vp, vp, vp, vp, sz, vp]
         L.luthe_blind_rotate.argtypes = [vp, vp, vp, vp, sz, vp]
         L.luthe_ntt_fwd.argtypes = [vp, vp, vp, sz, vp]
@@ -389,6 +390,11 @@ class Server:
             return None
         _check(code)
         return out, lat.value, q.value
+
+    def set_batching(self, fill=0, window_us=0):
+        """Hold ready PBS DOps while a lane is busy, fewer than `fill` are
+        ready and the oldest waited less than `window_us` (0: off)."""
+        _check(lib().luthe_server_set_batching(self._h, fill, window_us))
 
     def counters(self):
         v = [ctypes.c_uint64() for _ in range(4)]

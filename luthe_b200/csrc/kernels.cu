@@ -436,6 +436,11 @@ __device__ __forceinline__ bool group_sync_or(int bar_id, bool pred)
     return r != 0;
 }
 
+// Output BLWEs are written once and not read again by this launch: a
+// streaming (evict-first) store keeps them from pushing the BSK, which every
+// CTA re-reads at every step, out of L2.
+__device__ __forceinline__ void st_stream(u64 *p, u64 v) { __stcs(reinterpret_cast<unsigned long long *>(p), v); }
+
 __device__ __forceinline__ void issue_slab(u64 *slab, const u64 *src, u64 *mbar)
 {
     mbar_expect_tx(mbar, (u32)SLAB_BYTES);
@@ -632,11 +637,11 @@ __global__ void __launch_bounds__(G * 256, 1)
                     const u32 src = (j + b) & (TWO_N - 1);
                     u64 v = bp[src & (N - 1)];
                     if (src >= (u32)N) v = 0ull - v;
-                    o[oi] = oi == 0 ? v : 0ull - v;
+                    st_stream(o + oi, oi == 0 ? v : 0ull - v);
                 }
                 if (t == 0) {
                     u64 v = bp[POLY_WORDS + (b & (N - 1))];
-                    o[N] = b >= (u32)N ? 0ull - v : v;
+                    st_stream(o + N, b >= (u32)N ? 0ull - v : v);
                 }
             }
         }
@@ -797,11 +802,11 @@ __global__ void __launch_bounds__(512, 1)
                 const u32 src = (j + b) & (TWO_N - 1);
                 u64 v = bp0[src & (N - 1)];
                 if (src >= (u32)N) v = 0ull - v;
-                o[oi] = oi == 0 ? v : 0ull - v;
+                st_stream(o + oi, oi == 0 ? v : 0ull - v);
             }
             if (threadIdx.x == 0) {
                 u64 v = bp1[b & (N - 1)];
-                o[N] = b >= (u32)N ? 0ull - v : v;
+                st_stream(o + N, b >= (u32)N ? 0ull - v : v);
             }
         }
         __syncthreads();
@@ -974,11 +979,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                     const u32 src = (j + b) & (TWO_N - 1);
                     u64 v = bp[src & (N - 1)];
                     if (src >= (u32)N) v = 0ull - v;
-                    o[oi] = oi == 0 ? v : 0ull - v;
+                    st_stream(o + oi, oi == 0 ? v : 0ull - v);
                 }
             } else if (t == 0) {
                 u64 v = bp[b & (N - 1)];
-                o[N] = b >= (u32)N ? 0ull - v : v;
+                st_stream(o + N, b >= (u32)N ? 0ull - v : v);
             }
         }
         __syncthreads();

@@ -48,6 +48,7 @@ struct Instr {
     int npred = 0;
     std::vector<int> succ;
     bool done = false;
+    std::chrono::steady_clock::time_point t_ready;  // when its last dependency finished
 };
 
 using clock_t_ = std::chrono::steady_clock;
@@ -185,8 +186,12 @@ void build_dag(Request &r)
     for (auto &in : r.prog)
         for (int s : in.succ) r.prog[s].npred++;
     r.ready.clear();
+    const auto now = clock_t_::now();
     for (int i = 0; i < (int)r.prog.size(); i++)
-        if (r.prog[i].npred == 0) r.ready.push_back(i);
+        if (r.prog[i].npred == 0) {
+            r.prog[i].t_ready = now;
+            r.ready.push_back(i);
+        }
     r.remaining = r.prog.size();
 }
 
@@ -258,6 +263,10 @@ struct luthe_server {
     uint32_t ops_cap = 0, ops_head = 0;
     uint32_t max_pbs = 4096;
     uint64_t rounds = 0, pbs_done = 0, alu_done_n = 0, launches = 0;
+    // batching window (luthe_server_set_batching): 0 = off
+    uint32_t fill = 0;
+    double window_s = 0;
+    uint64_t held = 0;  // rounds in which ready PBS were held back
 };
 
 namespace {
@@ -275,7 +284,10 @@ void finish(Request *r, int i)
     r->prog[i].done = true;
     r->remaining--;
     for (int j : r->prog[i].succ)
-        if (--r->prog[j].npred == 0) r->ready.push_back(j);
+        if (--r->prog[j].npred == 0) {
+            r->prog[j].t_ready = clock_t_::now();
+            r->ready.push_back(j);
+        }
 }
 
 }  // namespace
@@ -504,11 +516,31 @@ extern "C" int luthe_server_step(luthe_server *s, uint32_t *n_completed, uint32_
     // ready PBS on idle lanes (one many-LUT factor per batch)
     for (Lane &ln : s->lanes) {
         if (ln.busy) continue;
-        uint32_t mlk = 0, B = 0;
+        uint32_t mlk = 0, B = 0, nready = 0;
+        clock_t_::time_point oldest = clock_t_::time_point::max();
         for (Request *r : s->active)
             for (int i : r->ready)
-                if (r->prog[i].kind == 1 && !mlk) mlk = r->prog[i].mlk;
+                if (r->prog[i].kind == 1) {
+                    if (!mlk) mlk = r->prog[i].mlk;
+                    if (r->prog[i].mlk == mlk) {
+                        nready++;
+                        oldest = std::min(oldest, r->prog[i].t_ready);
+                    }
+                }
         if (!mlk) break;
+        if (s->window_s > 0) {
+            // the HPU's batch policy: a batch leaves when full or when its
+            // oldest entry has waited the timeout; while the GPU is idle there
+            // is nothing to wait for
+            bool any_busy = false;
+            for (const Lane &o : s->lanes) any_busy |= o.busy;
+            const uint32_t fill = s->fill ? s->fill : 2u * (uint32_t)c->nsm;
+            const double waited = std::chrono::duration<double>(clock_t_::now() - oldest).count();
+            if (any_busy && nready < fill && waited < s->window_s) {
+                s->held++;
+                break;
+            }
+        }
         for (Request *r : s->active) {
             std::vector<int> keep;
             for (int i : r->ready) {
@@ -558,6 +590,15 @@ extern "C" int luthe_server_fetch(luthe_server *s, uint64_t id, uint64_t *h_dst,
     s->host.release(r->hbase, r->n_src + r->n_dst);
     s->done.erase(it);
     delete r;
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_server_set_batching(luthe_server *s, uint32_t fill, uint32_t window_us)
+{
+    if (!s) return fail(LUTHE_E_PARAM, "null server");
+    if (fill > s->max_pbs) return fail(LUTHE_E_PARAM, "fill %u exceeds the server's batch limit %u", fill, s->max_pbs);
+    s->fill = fill;
+    s->window_s = window_us * 1e-6;
     return LUTHE_OK;
 }
 

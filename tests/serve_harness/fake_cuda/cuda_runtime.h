@@ -53,13 +53,29 @@ static inline cudaError_t cudaStreamDestroy(cudaStream_t s)
 }
 static inline cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
 static inline cudaError_t cudaStreamWaitEvent(cudaStream_t, cudaEvent_t, unsigned) { return cudaSuccess; }
+// Events: an event recorded reports "not ready" for the next g_fake_event_lag
+// queries (0 by default: work is complete as soon as it is enqueued), so that
+// tests can keep PBS lanes busy across scheduler steps.
+static int g_fake_event_lag = 0;
 static inline cudaError_t cudaEventCreateWithFlags(cudaEvent_t *e, unsigned)
 {
-    *e = (cudaEvent_t)malloc(1);
+    *e = (cudaEvent_t)calloc(1, sizeof(int));
     return cudaSuccess;
 }
-static inline cudaError_t cudaEventRecord(cudaEvent_t, cudaStream_t) { return cudaSuccess; }
-static inline cudaError_t cudaEventQuery(cudaEvent_t) { return cudaSuccess; }
+static inline cudaError_t cudaEventRecord(cudaEvent_t e, cudaStream_t)
+{
+    *(int *)e = g_fake_event_lag;
+    return cudaSuccess;
+}
+static inline cudaError_t cudaEventQuery(cudaEvent_t e)
+{
+    int *left = (int *)e;
+    if (*left > 0) {
+        --*left;
+        return cudaErrorNotReady;
+    }
+    return cudaSuccess;
+}
 static inline cudaError_t cudaEventDestroy(cudaEvent_t e)
 {
     free(e);

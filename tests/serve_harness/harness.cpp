@@ -88,6 +88,8 @@ extern "C" luthe_ctx *harness_ctx(uint32_t n, const uint64_t *tables, uint32_t n
     memcpy(c->d_luts, tables, (size_t)nlut * 16 * 8);
     return c;
 }
+extern "C" void harness_set_event_lag(int polls) { g_fake_event_lag = polls; }
+
 extern "C" void harness_ctx_free(luthe_ctx *c)
 {
     free(c->d_err);

@@ -30,6 +30,9 @@ def H():
     lib.luthe_server_submit.argtypes = [vp, vp, u32, vp, u32, u32, ctypes.POINTER(u64)]
     lib.luthe_server_step.argtypes = [vp] + [ctypes.POINTER(u32)] * 3
     lib.luthe_server_fetch.argtypes = [vp, u64, vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.luthe_server_set_batching.argtypes = [vp, u32, u32]
+    lib.luthe_server_counters.argtypes = [vp] + [ctypes.POINTER(u64)] * 4
+    lib.harness_set_event_lag.argtypes = [ctypes.c_int]
     return lib
 
 
@@ -138,3 +141,56 @@ def test_bad_programs_are_rejected(H):
     rc, _ = s.submit(np.array([I.enc_pbs("PBS_ML2", 3, 1, 0)], np.uint32), [], 1)
     assert rc != 0                                          # many-LUT destination not aligned
     s.close()
+
+
+def _mixed(rng, n):
+    reqs, expect = [], []
+    for r in range(n):
+        a, b = rng.randrange(65536), rng.randrange(65536)
+        if r % 2:
+            reqs.append((I.prog_add(), I.to_blocks(a) + I.to_blocks(b), 8))
+            expect.append((a + b) % 65536)
+        else:
+            reqs.append((I.prog_mul(), I.to_blocks(a) + I.to_blocks(b), 8))
+            expect.append((a * b) % 65536)
+    return reqs, expect
+
+
+def run_staggered(s, reqs):
+    """Submit one request per scheduler step (arrivals spread over time)."""
+    ids, outs = [], {}
+    for _ in range(20000):
+        if len(ids) < len(reqs):
+            rc, rid = s.submit(*reqs[len(ids)])
+            assert rc == 0
+            ids.append(rid)
+        s.step()
+        for k, rid in enumerate(ids):
+            if k not in outs:
+                got = s.fetch(rid, reqs[k][2])
+                if got is not None:
+                    outs[k] = got
+        if len(outs) == len(reqs):
+            break
+    return [outs[k] for k in range(len(reqs))]
+
+
+def test_batching_window_holds_partial_batches_and_stays_correct(H):
+    """With lanes busy across steps (events lag), a batching window makes the
+    scheduler hold partial PBS batches: fewer, larger launches, same results."""
+    launches = {}
+    for window in (0, 10_000_000):
+        H.harness_set_event_lag(3)
+        try:
+            s = PlainServer(H, 1 << 15)
+            assert H.luthe_server_set_batching(s.srv, 64, window) == 0
+            reqs, expect = _mixed(random.Random(11), 24)
+            outs = run_staggered(s, reqs)
+            cnt = [u64() for _ in range(4)]
+            H.luthe_server_counters(s.srv, *[ctypes.byref(x) for x in cnt])
+            launches[window] = cnt[0].value  # PBS rounds (one KS+PBS launch each)
+            s.close()
+        finally:
+            H.harness_set_event_lag(0)
+        assert [I.from_blocks(o) for o in outs] == expect
+    assert launches[10_000_000] < launches[0]
