@@ -101,30 +101,33 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def _profile_values(name, keys):
-    path = os.path.join(ROOT, "profiles", name)
-    vals = {}
-    if os.path.exists(path):
-        for line in open(path):
-            k, _, v = line.partition(":")
-            if k.strip() in keys:
-                vals[k.strip()] = float(v)
-    return vals
+def ncu_record():
+    """The ncu figures of the blind-rotation kernel kept in
+    profiles/br_kernel_ncu.json (written from an ncu capture; it names the
+    commit and the command it was captured with), or None."""
+    path = os.path.join(ROOT, "profiles", "br_kernel_ncu.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
 
 
-def read_traffic(B):
+def read_traffic(B, rec):
     """DRAM bytes (read + write) of one blind-rotation launch over B
-    ciphertexts: the ncu figure of the bench's own full-size launch
-    (profiles/br_kernel_traffic.md) when it was taken at this B, else the
-    296-ciphertext capture (profiles/br_kernel_ncu.md) scaled as the BSK read
-    once per launch plus the per-ciphertext bytes.  Returns (bytes, how)."""
-    full = _profile_values("br_kernel_traffic.md", ("ciphertexts_per_launch", "dram_bytes_per_launch"))
-    if full.get("ciphertexts_per_launch") == B and "dram_bytes_per_launch" in full:
-        return full["dram_bytes_per_launch"], "ncu, this launch size"
-    small = _profile_values("br_kernel_ncu.md", ("dram_bytes_fixed_per_launch", "dram_bytes_per_bootstrap"))
-    if len(small) < 2:
+    ciphertexts from the ncu record: the capture of a launch of this size when
+    there is one, else the one-wave capture scaled as the BSK read once per
+    launch plus the per-ciphertext bytes.  Returns (bytes, how)."""
+    if not rec:
         return None, None
-    return small["dram_bytes_fixed_per_launch"] + small["dram_bytes_per_bootstrap"] * B, "ncu, scaled from 296"
+    for cap in rec.get("captures", []):
+        if cap.get("ciphertexts") == B and cap.get("dram_bytes"):
+            return cap["dram_bytes"], f"ncu, a launch of {B} ciphertexts (commit {rec.get('commit')})"
+    scale = rec.get("traffic_model")
+    if scale:
+        return (scale["fixed_bytes"] + scale["bytes_per_ciphertext"] * B,
+                f"ncu, scaled from the {scale.get('from')}-ciphertext capture (commit {rec.get('commit')})")
+    return None, None
 
 
 class _OracleHost:
@@ -504,8 +507,8 @@ def main():
     br_s = statistics.median(br_ms) * 1e-3
     imad_peak, glmul_peak = L.measure_int_peak(local)
     achieved_imad = B * MODMUL_PER_BOOTSTRAP * IMAD_PER_MODMUL / br_s
-    traffic, traffic_how = read_traffic(B)
-    pipes = _profile_values("br_kernel_ncu.md", ("alu_pipe_busy", "fma_pipe_busy", "issue_active"))
+    ncu = ncu_record()
+    traffic, traffic_how = read_traffic(B, ncu)
 
     # ---- plain path: one ciphertext per launch
     plain_ms = []
@@ -655,8 +658,8 @@ def main():
                          "traffic": traffic, "traffic_unit": f"DRAM bytes per launch ({traffic_how})",
                          "modmul_frac": B * MODMUL_PER_BOOTSTRAP / br_s / glmul_peak,
                          "glmul_peak_per_s": glmul_peak, "br_ms": br_s * 1e3,
-                         "pipe_utilisation_ncu": dict(pipes, source="profiles/br_kernel_ncu.md (296-BLWE wave)")
-                         if pipes else None},
+                         "ncu": ncu and {k: ncu.get(k) for k in ("commit", "kernel", "command", "pipes", "l2",
+                                                                   "warp_instructions_per_ciphertext_step")}},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(ct.nbytes + ids.nbytes),
                     "d2h_bytes_per_step": int(ct.nbytes), "ms_per_step": statistics.mean(e2e_ms)},

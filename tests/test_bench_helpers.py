@@ -1,6 +1,6 @@
 """Host logic of bench.py on the CPU: the blind-rotation launch count it
 reports (mirroring launch_blind_rotate's shapes), the DRAM-traffic lookup from
-the committed ncu summaries, and the CPU baselines of the NTT-product and
+the committed ncu record, and the CPU baselines of the NTT-product and
 key-switch configurations against the oracle."""
 import numpy as np
 
@@ -21,10 +21,14 @@ def test_blind_rotation_launches_per_step():
 
 
 def test_traffic_lookup():
-    full, how = bench.read_traffic(5370)
-    assert how == "ncu, this launch size" and 1e8 < full < 1e9
-    small, how = bench.read_traffic(296)
-    assert how == "ncu, scaled from 296" and 5e7 < small < full
+    rec = {"commit": "abc", "captures": [{"ciphertexts": 5370, "dram_bytes": 1.6e8}],
+           "traffic_model": {"from": 296, "fixed_bytes": 5.3e7, "bytes_per_ciphertext": 1.7e4}}
+    full, how = bench.read_traffic(5370, rec)
+    assert full == 1.6e8 and "5370" in how and "abc" in how
+    small, how = bench.read_traffic(296, rec)
+    assert small == 5.3e7 + 1.7e4 * 296 and "scaled" in how
+    assert bench.read_traffic(296, None) == (None, None)
+    assert bench.br_launches_per_step(5370, 148, 2, tail_max=0) == 1  # tuned: the tail stays in the wave launch
 
 
 def test_cpu_baselines_are_bit_checked():
