@@ -17,6 +17,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_autotune_choice_is_saved_loaded_and_exact(engine, params, keys, oracle_bsk, tmp_path):
+    rng = np.random.default_rng(5)
+    table = rng.integers(0, 16, 16).astype(np.uint32)
+    luts = L.lut_build(params, table)[None, :]
+    engine.upload_luts(luts)
     rec = engine.autotune(0)
     chosen = rec["chosen"]
     assert chosen["format"] == "luthe-tuning-1" and chosen["cts_per_cta"] in (1, 2)
@@ -45,12 +49,8 @@ def test_autotune_choice_is_saved_loaded_and_exact(engine, params, keys, oracle_
         engine.tuning_load(bad)
     engine.tuning_load(path)
     # the tuned shape computes the same outputs as the oracle
-    rng = np.random.default_rng(5)
     count = 2 * 148 + 60
     msgs = rng.integers(0, 16, count).astype(np.uint32)
-    table = rng.integers(0, 16, 16).astype(np.uint32)
-    luts = L.lut_build(params, table)[None, :]
-    engine.upload_luts(luts)
     ct = L.encrypt(params, keys["glwe_key"], msgs, 55)
     ids = np.zeros(count, np.uint32)
     d_out = to_dev(np.zeros_like(ct))
