@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--no-param-sets", action="store_true",
                     help="skip the KS+PBS measurement of the reference's other parameter sets")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shape (profiling runs: no tuning trials among the launches)")
     ap.add_argument("--ncu-case", action="store_true",
                     help="small profiling case: KS+PBS of 296 BLWEs (one persistent wave), twice, then exit")
     return ap.parse_args()
@@ -442,7 +444,7 @@ def main():
     eng = L.Engine(params, device=local)
     eng.upload_keys(keys)
     eng.upload_luts(luts)
-    tune = eng.autotune(0)
+    tune = {"chosen": None, "skipped": "--no-autotune"} if args.no_autotune else eng.autotune(0)
     eng.reserve(B)
 
     d_in = torch.from_numpy(ct.view(np.int64)).cuda()
