@@ -396,12 +396,21 @@ __device__ __forceinline__ void mbar_expect_tx(u64 *mbar, u32 bytes)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)), "r"(bytes)
                  : "memory");
 }
+// BSK slabs are re-read by every CTA at every step of every wave: they are
+// fetched with an L2 evict-last policy so that the output BLWEs streaming
+// through L2 do not push them out between waves.
+__device__ __forceinline__ u64 bsk_l2_policy()
+{
+    u64 pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, u32 bytes, u64 *mbar)
 {
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
             smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+        "l"(src), "r"(bytes), "r"(smem_addr(mbar)), "l"(bsk_l2_policy())
         : "memory");
 }
 // bounded wait on the given phase parity; returns false after `polls` polls
