@@ -66,3 +66,23 @@ def test_bsk_loader_checks_its_input():
         pass
     else:
         raise AssertionError("a BSK of the wrong size was accepted")
+
+
+def test_bsk_points_relabel_for_another_root():
+    """A file written for another primitive 2N-th root phi = psi^u holds
+    A(phi^(2k+1)) = A(psi^(2k'+1)): the importer's map sends k to k'."""
+    P = 2**64 - 2**32 + 1
+    for N in (64, 2048):
+        psi = pow(H.PSI_4096, 2048 // N, P)
+        for u in (1, 3, 2 * N - 1):
+            phi = pow(psi, u, P)
+            kmap = H._point_map(N, phi)
+            assert sorted(kmap.tolist()) == list(range(N))
+            for k in (0, 1, N // 2, N - 1):
+                assert pow(phi, 2 * k + 1, P) == pow(psi, 2 * int(kmap[k]) + 1, P)
+    try:
+        H._point_map(64, 2)  # 2 is not a primitive 128-th root
+    except ValueError:
+        pass
+    else:
+        raise AssertionError("a wrong root was accepted")
