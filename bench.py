@@ -124,7 +124,7 @@ def read_traffic(B, rec):
         return None, None
     for cap in rec.get("captures", []):
         if cap.get("ciphertexts") == B and cap.get("dram_bytes"):
-            return cap["dram_bytes"], f"ncu, a launch of {B} ciphertexts (commit {rec.get('commit')})"
+            return cap["dram_bytes"], f"ncu, a launch of {B} ciphertexts (commit {cap.get('commit', rec.get('commit'))})"
     scale = rec.get("traffic_model")
     if scale:
         return (scale["fixed_bytes"] + scale["bytes_per_ciphertext"] * B,
