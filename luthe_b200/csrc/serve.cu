@@ -559,17 +559,10 @@ extern "C" int luthe_server_step(luthe_server *s, uint32_t *n_completed, uint32_
             }
             r->ready.swap(keep);
         }
-        // Under load the GPU is full anyway: small batches then use one
-        // ciphertext per CTA (96 bootstraps/s per SM) rather than a 2-SM
-        // cluster each (69/s per SM, lower latency only on an idle GPU).
-        BrConfig cfg = c->br;
-        int busy = 0;
-        for (const Lane &o : s->lanes) busy += o.busy;
-        if (busy >= LANES / 2) cfg.pair_max = 0;
         CUDA_TRY(cudaStreamWaitEvent(ln.stream, s->alu_done, 0));
         CUDA_TRY(cudaMemcpyAsync(ln.d_idx, ln.h_idx, (size_t)s->max_pbs * 3 * 4, cudaMemcpyHostToDevice, ln.stream));
         CUDA_TRY(launch_keyswitch(s->d_pool, c->d_ksk, nullptr, ln.d_l2n, B, n, c->xpad, ln.stream, ln.d_idx, c->p.ks_base_log, c->p.ks_level, c->tie_rule));
-        CUDA_TRY(launch_blind_rotate(cfg, c->nsm, ln.d_l2n, c->d_luts, ln.d_idx + 2 * s->max_pbs, c->nlut,
+        CUDA_TRY(launch_blind_rotate(c->br, c->nsm, ln.d_l2n, c->d_luts, ln.d_idx + 2 * s->max_pbs, c->nlut,
                                      c->d_bsk, c->d_tw, s->d_pool, B, n, c->d_err, ln.stream,
                                      ln.d_idx + s->max_pbs, mlk, c->p.pbs_base_log, c->tie_rule));
         CUDA_TRY(cudaEventRecord(ln.done, ln.stream));
