@@ -75,3 +75,35 @@ def test_host_entry_point(setup):
     assert np.array_equal(out, ob.ks_pbs(keys["ksk"], ct, luts, np.zeros(16, np.uint32), ks_bl=p.ks_base_log,
                                          ks_lc=p.ks_level, pbs_bl=p.pbs_base_log)), name
     assert [int(x) for x in L.decrypt(p, keys["glwe_key"], out)] == [15 - m for m in range(16)]
+
+
+def test_generator_tie_rule_matches_oracle(setup):
+    """Each set's key switch (2x8, 2x7, 3x5 decompositions) and blind rotation
+    (2^23 or 2^22) in the reference generator's tie rule, against the oracle
+    in the same rule; the rule changes the top digits of most ciphertexts."""
+    name, p, keys, eng, ob = setup
+    rng = np.random.default_rng(31 + p.lwe_dim)
+    table = rng.integers(0, 16, 16).astype(np.uint32)
+    luts = L.lut_build(p, table)[None]
+    count = 24
+    msgs = rng.integers(0, 16, count).astype(np.uint32)
+    ids = np.zeros(count, np.uint32)
+    ct = L.encrypt(p, keys["glwe_key"], msgs, 77 + p.lwe_dim)
+    eng.upload_luts(luts)
+    d_rtl, d_gen = to_dev(np.zeros((count, N + 1), np.uint64)), to_dev(np.zeros((count, N + 1), np.uint64))
+    eng.ks_pbs(to_dev(ct), to_dev(ids), d_rtl, count)
+    eng.set_tie_rule(L.TIE_GENERATOR)
+    try:
+        eng.ks_pbs(to_dev(ct), to_dev(ids), d_gen, count)
+        eng.check_device_error()
+    finally:
+        eng.set_tie_rule(L.TIE_RTL)
+    got = from_dev(d_gen, np.uint64)
+    oracle.set_tie_rule(True)
+    try:
+        want = ob.ks_pbs(keys["ksk"], ct, luts, ids, ks_bl=p.ks_base_log, ks_lc=p.ks_level, pbs_bl=p.pbs_base_log)
+    finally:
+        oracle.set_tie_rule(False)
+    assert np.array_equal(got, want), name
+    assert not np.array_equal(got, from_dev(d_rtl, np.uint64)), name
+    assert [int(x) for x in L.decrypt(p, keys["glwe_key"], got)] == [int(table[m]) for m in msgs], name
