@@ -134,6 +134,7 @@ extern "C" void luthe_ctx_destroy(luthe_ctx *c)
     dfree(c, c->d_err, 4);
     dfree(c, c->d_bsk, n * SLAB_BYTES);
     dfree(c, c->d_ksk, (size_t)N * c->p.ks_level * c->xpad * 4);
+    dfree(c, c->d_ks_part, (size_t)KS_BM * c->xpad * 4);
     dfree(c, c->d_luts, (size_t)c->nlut * 2 * N * 8);
     dfree(c, c->d_lwe2N, c->cap * (n + 1) * 4);
     dfree(c, c->d_hin, c->hcap * (N + 1) * 8);
@@ -215,6 +216,8 @@ extern "C" int luthe_upload_ksk(luthe_ctx *c, const uint32_t *h)
     if (!c->d_ksk) {
         if ((r = dalloc(c, (void **)&c->d_ksk, K * xpad * 4))) return r;
         c->xpad = xpad;
+        if ((r = dalloc(c, (void **)&c->d_ks_part, (size_t)KS_BM * xpad * 4))) return r;
+        CUDA_TRY(cudaMemset(c->d_ks_part, 0, (size_t)KS_BM * xpad * 4));
     }
     CUDA_TRY(cudaMemcpy(c->d_ksk, t.data(), K * xpad * 4, cudaMemcpyHostToDevice));
     return LUTHE_OK;
@@ -268,7 +271,8 @@ static int enqueue_ks_pbs(luthe_ctx *c, const uint64_t *d_in, const uint32_t *d_
                           cudaStream_t s)
 {
     const uint32_t n = c->p.lwe_dim;
-    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level, c->tie_rule));
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr, c->p.ks_base_log,
+                              c->p.ks_level, c->tie_rule, c->d_ks_part));
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out,
                                  count, n, c->d_err, s, nullptr, 1, c->p.pbs_base_log, c->tie_rule));
     return LUTHE_OK;
@@ -298,7 +302,8 @@ extern "C" int luthe_ks_pbs_ml(luthe_ctx *c, const uint64_t *d_in, const uint32_
     if ((r = ensure_scratch(c, count))) return r;
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t n = c->p.lwe_dim;
-    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level, c->tie_rule));
+    CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr, c->p.ks_base_log,
+                              c->p.ks_level, c->tie_rule, c->d_ks_part));
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, d_ids, c->nlut, c->d_bsk, c->d_tw, d_out, count,
                                  n, c->d_err, s, nullptr, mlk, c->p.pbs_base_log, c->tie_rule));
     return LUTHE_OK;
@@ -382,7 +387,8 @@ extern "C" int luthe_keyswitch(luthe_ctx *c, const uint64_t *d_in, uint32_t *d_o
     if (!d_in || !d_out2N) return fail(LUTHE_E_PARAM, "null buffer");
     CUDA_TRY(cudaSetDevice(c->device));
     CUDA_TRY(launch_keyswitch(d_in, c->d_ksk, d_out21, d_out2N, count, c->p.lwe_dim, c->xpad,
-                              (cudaStream_t)stream, nullptr, c->p.ks_base_log, c->p.ks_level, c->tie_rule));
+                              (cudaStream_t)stream, nullptr, c->p.ks_base_log, c->p.ks_level, c->tie_rule,
+                              c->d_ks_part));
     return LUTHE_OK;
 }
 

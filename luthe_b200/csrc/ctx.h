@@ -23,6 +23,7 @@ struct luthe_ctx {
     uint64_t *d_bsk = nullptr;    // [n][8][2][2][256]
     uint32_t *d_ksk = nullptr;    // [kN*L][xpad]
     uint32_t xpad = 0;
+    uint32_t *d_ks_part = nullptr;  // [KS_BM][xpad] split-K partial sums of small key switches (kept zero)
     uint64_t *d_luts = nullptr;   // [nlut][2][N]
     uint32_t nlut = 0;
     uint32_t *d_err = nullptr;

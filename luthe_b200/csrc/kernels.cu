@@ -266,7 +266,8 @@ __device__ __forceinline__ void ks_decomp(u64 v, int *d)
 template <int BL, int L, bool GEN>
 __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, const u32 *__restrict__ src_idx,
                                                   const u32 *__restrict__ ksk_t, u32 *__restrict__ out21,
-                                                  u32 *__restrict__ out2N, u32 B, u32 n, u32 xpad)
+                                                  u32 *__restrict__ out2N, u32 B, u32 n, u32 xpad,
+                                                  u32 *__restrict__ part)
 {
     __shared__ __align__(16) int dsm[KS_KC * L][KS_BM];  // digits [k][ct]
     __shared__ __align__(16) u32 ksm[KS_KC * L][KS_BN];  // KSK tile [k][x]
@@ -282,7 +283,10 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
     const int dct = tid >> 3, dy = tid & 7;  // decomposition role: 32 cts x 8 coefs
     const u32 dct_c = min(c0 + dct, B - 1);
     const size_t dct_g = src_idx ? src_idx[dct_c] : dct_c;  // row of the input array
-    for (u32 y0 = 0; y0 < (u32)N; y0 += KS_KC) {
+    // split-K (gridDim.z > 1, small batches): this CTA sums its slice of the
+    // mask coefficients and adds the partial sums into `part`
+    const u32 span = (u32)N / gridDim.z, y_lo = blockIdx.z * span;
+    for (u32 y0 = y_lo; y0 < y_lo + span; y0 += KS_KC) {
         {
             int d[L];
             ks_decomp<BL, L, GEN>(in[(size_t)dct_g * (N + 1) + y0 + dy], d);
@@ -310,6 +314,20 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
         }
         __syncthreads();
     }
+    if (part) {
+        // 32-bit wrap-around sums are exact mod 2^21 in any order
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const u32 c = c0 + ty * 4 + i;
+            if (c >= B) continue;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const u32 x = x0 + tx * 4 + j;
+                if (x <= n) atomicAdd(&part[(size_t)c * xpad + x], acc[i][j]);
+            }
+        }
+        return;
+    }
     const u32 M = (1u << KS_W) - 1;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -333,29 +351,61 @@ bool ks_supported(uint32_t bl, uint32_t L)
     return (bl == 3 && (L == 6 || L == 5)) || (bl == 2 && (L == 8 || L == 7));
 }
 
+// The split-K form's epilogue: out = [x == n] b21 - sum (mod 2^21) and its 2N
+// switch, as ks_kernel's own epilogue; the partial sums are cleared behind
+// it, so `part` is zero again for the next call.
+__global__ void __launch_bounds__(256) ks_finish(const u64 *__restrict__ in, const u32 *__restrict__ src_idx,
+                                                  u32 *__restrict__ part, u32 *__restrict__ out21,
+                                                  u32 *__restrict__ out2N, u32 B, u32 n, u32 xpad)
+{
+    const u32 M = (1u << KS_W) - 1;
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < B * (n + 1); i += gridDim.x * blockDim.x) {
+        const u32 c = i / (n + 1), x = i % (n + 1);
+        u32 *pp = &part[(size_t)c * xpad + x];
+        u32 v = (0u - *pp) & M;
+        *pp = 0;
+        if (x == n) {
+            const u64 b = in[(size_t)(src_idx ? src_idx[c] : c) * (N + 1) + N];
+            v = (v + (u32)((b >> (64 - KS_W)) + ((b >> (63 - KS_W)) & 1ull))) & M;
+        }
+        if (out21) out21[(size_t)c * (n + 1) + x] = v;
+        out2N[(size_t)c * (n + 1) + x] = ((v >> 9) + ((v >> 8) & 1u)) & (TWO_N - 1);
+    }
+}
+
 template <bool GEN>
 static cudaError_t launch_keyswitch_rule(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21,
                                          uint32_t *d_out2N, u32 B, uint32_t n, uint32_t xpad, cudaStream_t s,
-                                         const uint32_t *d_src_idx, uint32_t bl, uint32_t L)
+                                         const uint32_t *d_src_idx, uint32_t bl, uint32_t L, uint32_t *d_part)
 {
-    dim3 grid(xpad / KS_BN, (B + KS_BM - 1) / KS_BM);
-    if (bl == 3 && L == 6) ks_kernel<3, 6, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad);
-    else if (bl == 3 && L == 5) ks_kernel<3, 5, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad);
-    else if (bl == 2 && L == 8) ks_kernel<2, 8, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad);
-    else if (bl == 2 && L == 7) ks_kernel<2, 7, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad);
+    // one ciphertext tile: split the mask coefficients over KS_SPLIT CTAs per
+    // output tile (a tile walks all 256 coefficient chunks in sequence otherwise)
+    const bool split = d_part && B <= (u32)KS_BM;
+    dim3 grid(xpad / KS_BN, (B + KS_BM - 1) / KS_BM, split ? KS_SPLIT : 1);
+    u32 *part = split ? d_part : nullptr;
+    if (bl == 3 && L == 6) ks_kernel<3, 6, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad, part);
+    else if (bl == 3 && L == 5) ks_kernel<3, 5, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad, part);
+    else if (bl == 2 && L == 8) ks_kernel<2, 8, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad, part);
+    else if (bl == 2 && L == 7) ks_kernel<2, 7, GEN><<<grid, 256, 0, s>>>(d_in, d_src_idx, d_ksk_t, d_out21, d_out2N, B, n, xpad, part);
     else return cudaErrorInvalidValue;
+    if (split) {
+        const u32 total = B * (n + 1);
+        ks_finish<<<(total + 255) / 256, 256, 0, s>>>(d_in, d_src_idx, d_part, d_out21, d_out2N, B, n, xpad);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21, uint32_t *d_out2N,
                              size_t B, uint32_t n, uint32_t xpad, cudaStream_t s, const uint32_t *d_src_idx,
-                             uint32_t bl, uint32_t L, uint32_t tie_rule)
+                             uint32_t bl, uint32_t L, uint32_t tie_rule, uint32_t *d_part)
 {
     if (B == 0) return cudaSuccess;
     if (tie_rule == TIE_GENERATOR)
-        return launch_keyswitch_rule<true>(d_in, d_ksk_t, d_out21, d_out2N, (u32)B, n, xpad, s, d_src_idx, bl, L);
+        return launch_keyswitch_rule<true>(d_in, d_ksk_t, d_out21, d_out2N, (u32)B, n, xpad, s, d_src_idx, bl, L,
+                                           d_part);
     if (tie_rule != TIE_RTL) return cudaErrorInvalidValue;
-    return launch_keyswitch_rule<false>(d_in, d_ksk_t, d_out21, d_out2N, (u32)B, n, xpad, s, d_src_idx, bl, L);
+    return launch_keyswitch_rule<false>(d_in, d_ksk_t, d_out21, d_out2N, (u32)B, n, xpad, s, d_src_idx, bl, L,
+                                        d_part);
 }
 
 // ---------------------------------------------------------- blind rotation

@@ -14,6 +14,7 @@ constexpr int KS_W = 21;
 constexpr int KS_BN = 128;                    // key-switch output tile
 constexpr int KS_BM = 32;                     // key-switch ciphertext tile
 constexpr int KS_KC = 8;                      // BLWE mask coefficients per K chunk
+constexpr int KS_SPLIT = 16;                  // K slices of the split-K key switch (batches <= KS_BM)
 constexpr int SLAB_WORDS = 8 * 4 * 256;       // one BR step of BSK: 2x2 polys of 2048
 constexpr size_t SLAB_BYTES = SLAB_WORDS * 8; // 64 KiB
 
@@ -44,7 +45,10 @@ constexpr uint32_t TIE_RTL = 0, TIE_GENERATOR = 1;
 cudaError_t launch_keyswitch(const uint64_t *d_in, const uint32_t *d_ksk_t, uint32_t *d_out21, uint32_t *d_out2N,
                              size_t B, uint32_t n, uint32_t xpad, cudaStream_t s,
                              const uint32_t *d_src_idx = nullptr, uint32_t bl = KS_BL, uint32_t L = KS_L,
-                             uint32_t tie_rule = TIE_RTL);
+                             uint32_t tie_rule = TIE_RTL, uint32_t *d_part = nullptr);
+// d_part: KS_BM x xpad u32, all zero, for the split-K form of batches of at
+// most KS_BM ciphertexts (left zero again); nullptr: the one-pass form only.
+// Calls that overlap on the GPU must not share it.
 bool ks_supported(uint32_t bl, uint32_t L);
 bool pbs_supported(uint32_t bw);
 // Bound on the polls of each BSK-slab wait of the blind rotation on the

@@ -236,6 +236,7 @@ struct Lane {
     cudaEvent_t done = nullptr;
     uint32_t *d_l2n = nullptr;   // [max_pbs][n+1]
     uint32_t *d_idx = nullptr;   // [3][max_pbs]: src, dst, gid
+    uint32_t *d_part = nullptr;  // split-K partial sums of this lane's small key switches (kept zero)
     uint32_t *h_idx = nullptr;   // pinned staging of d_idx
     std::vector<std::pair<Request *, int>> ops;
     bool busy = false;
@@ -321,6 +322,8 @@ extern "C" int luthe_server_create(luthe_ctx *c, uint64_t pool_bytes, uint32_t m
     for (int l = 0; ok && l < LANES; l++) {
         Lane &ln = s->lanes[l];
         ok = !dalloc(c, (void **)&ln.d_l2n, (size_t)s->max_pbs * n1 * 4) &&
+             !dalloc(c, (void **)&ln.d_part, (size_t)KS_BM * c->xpad * 4) &&
+             cudaMemset(ln.d_part, 0, (size_t)KS_BM * c->xpad * 4) == cudaSuccess &&
              !dalloc(c, (void **)&ln.d_idx, (size_t)s->max_pbs * 3 * 4) &&
              cudaMallocHost((void **)&ln.h_idx, (size_t)s->max_pbs * 3 * 4) == cudaSuccess &&
              cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking) == cudaSuccess &&
@@ -349,6 +352,7 @@ extern "C" void luthe_server_destroy(luthe_server *s)
         if (ln.h_idx) cudaFreeHost(ln.h_idx);
         dfree(c, ln.d_l2n, ln.d_l2n ? (size_t)s->max_pbs * n1 * 4 : 0);
         dfree(c, ln.d_idx, ln.d_idx ? (size_t)s->max_pbs * 3 * 4 : 0);
+        dfree(c, ln.d_part, ln.d_part ? (size_t)KS_BM * c->xpad * 4 : 0);
     }
     if (s->alu_stream) cudaStreamDestroy(s->alu_stream);
     if (s->alu_done) cudaEventDestroy(s->alu_done);
@@ -561,7 +565,8 @@ extern "C" int luthe_server_step(luthe_server *s, uint32_t *n_completed, uint32_
         }
         CUDA_TRY(cudaStreamWaitEvent(ln.stream, s->alu_done, 0));
         CUDA_TRY(cudaMemcpyAsync(ln.d_idx, ln.h_idx, (size_t)s->max_pbs * 3 * 4, cudaMemcpyHostToDevice, ln.stream));
-        CUDA_TRY(launch_keyswitch(s->d_pool, c->d_ksk, nullptr, ln.d_l2n, B, n, c->xpad, ln.stream, ln.d_idx, c->p.ks_base_log, c->p.ks_level, c->tie_rule));
+        CUDA_TRY(launch_keyswitch(s->d_pool, c->d_ksk, nullptr, ln.d_l2n, B, n, c->xpad, ln.stream, ln.d_idx, c->p.ks_base_log, c->p.ks_level, c->tie_rule,
+                                  ln.d_part));
         CUDA_TRY(launch_blind_rotate(c->br, c->nsm, ln.d_l2n, c->d_luts, ln.d_idx + 2 * s->max_pbs, c->nlut,
                                      c->d_bsk, c->d_tw, s->d_pool, B, n, c->d_err, ln.stream,
                                      ln.d_idx + s->max_pbs, mlk, c->p.pbs_base_log, c->tie_rule));

@@ -31,6 +31,11 @@ static inline cudaError_t cudaMemcpyAsync(void *d, const void *s, size_t n, cuda
     memcpy(d, s, n);
     return cudaSuccess;
 }
+static inline cudaError_t cudaMemset(void *d, int v, size_t n)
+{
+    memset(d, v, n);
+    return cudaSuccess;
+}
 static inline cudaError_t cudaMallocHost(void **p, size_t n)
 {
     *p = malloc(n);

@@ -57,7 +57,7 @@ cudaError_t launch_alu_batch(const AluOp *ops, uint64_t *pool, uint32_t nops, ui
     return cudaSuccess;
 }
 cudaError_t launch_keyswitch(const uint64_t *in, const uint32_t *, uint32_t *, uint32_t *out2N, size_t B, uint32_t n,
-                             uint32_t, cudaStream_t, const uint32_t *src_idx, uint32_t, uint32_t, uint32_t)
+                             uint32_t, cudaStream_t, const uint32_t *src_idx, uint32_t, uint32_t, uint32_t, uint32_t *)
 {
     for (size_t c = 0; c < B; c++) out2N[c * (n + 1)] = (uint32_t)in[(size_t)(src_idx ? src_idx[c] : c) * g_w];
     return cudaSuccess;
@@ -81,6 +81,7 @@ extern "C" luthe_ctx *harness_ctx(uint32_t n, const uint64_t *tables, uint32_t n
     luthe_ctx *c = new luthe_ctx();
     c->p.lwe_dim = n;
     c->p.poly_size = 2048;
+    c->xpad = 896;
     c->budget = budget;
     c->nlut = nlut;
     c->d_err = (uint32_t *)calloc(1, 4);

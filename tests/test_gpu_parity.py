@@ -78,6 +78,29 @@ def test_keyswitch_matches_oracle(engine, params, keys, count):
         assert np.array_equal(g2n[c], o2n), c
 
 
+def test_keyswitch_split_k_consecutive_calls(engine, params, keys):
+    """Batches of at most 32 ciphertexts switch keys in the split-K form (the
+    mask coefficients summed by 16 CTAs per output tile into a context buffer
+    that the finishing kernel leaves zero); calls in a row, both forms and
+    both tie rules, each equal to the oracle."""
+    n = params.lwe_dim
+    rng = np.random.default_rng(48)
+    for rule in (L.TIE_RTL, L.TIE_GENERATOR):
+        engine.set_tie_rule(rule)
+        try:
+            for count in (1, 5, 32, 33, 1):
+                blwe = rng.integers(0, 2**64, (count, N + 1), dtype=np.uint64)
+                d21 = to_dev(np.zeros((count, n + 1), np.uint32))
+                d2n = to_dev(np.zeros((count, n + 1), np.uint32))
+                engine.keyswitch(to_dev(blwe), d21, d2n, count)
+                g21, g2n = from_dev(d21, np.uint32), from_dev(d2n, np.uint32)
+                for c in range(count):
+                    o21, o2n = oracle.keyswitch(blwe[c], keys["ksk"], n, N, gtv_top_tie=rule == L.TIE_GENERATOR)
+                    assert np.array_equal(g21[c], o21) and np.array_equal(g2n[c], o2n), (rule, count, c)
+        finally:
+            engine.set_tie_rule(L.TIE_RTL)
+
+
 @pytest.mark.parametrize("g", [1, 2])
 def test_blind_rotate_matches_oracle(engine, params, oracle_bsk, g):
     rng = np.random.default_rng(50 + g)
