@@ -17,7 +17,10 @@
  *    the last failure on the calling thread is in luthe_last_error().  Errors
  *    are reported, never hidden: there is no CPU fallback.
  *  - A context is not thread-safe; one thread owns it (the HPU firmware loop
- *    is single-threaded too: fw/ublaze/src/ucore_fw.c:68).
+ *    is single-threaded too: fw/ublaze/src/ucore_fw.c:68).  Its calls share
+ *    the context's scratch (the key-switched intermediate, the split-K sums of
+ *    small key switches): calls of one context on different streams must be
+ *    ordered by the caller (events) or use separate contexts.
  *
  * Data formats (u64 torus values mod 2^64 unless stated)
  *  - BLWE: N mask coefficients in natural order, then the body
