@@ -49,8 +49,9 @@ def parse():
                     help="skip the KS+PBS measurement of the reference's other parameter sets")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shape (profiling runs: no tuning trials among the launches)")
-    ap.add_argument("--ncu-case", action="store_true",
-                    help="small profiling case: KS+PBS of 296 BLWEs (one persistent wave), twice, then exit")
+    ap.add_argument("--ncu-case", nargs="?", const="pbs", choices=("pbs", "other"),
+                    help="small profiling case, then exit: 'pbs' (default) KS+PBS of 296 BLWEs (one persistent "
+                         "wave), twice; 'other' the NTT product of 4096 pairs and the key switch of 16384 BLWEs, once each")
     return ap.parse_args()
 
 
@@ -418,10 +419,40 @@ def ncu_case():
     print("ncu case ok")
 
 
+def ncu_case_other():
+    """Configurations 1 and 3 once each at their full sizes (201 MB and 268 MB
+    of inputs): the NTT product of 4096 polynomial pairs and the key switch of
+    16384 BLWEs of dimension 2048, checked against the oracle on 4 rows."""
+    import torch
+    import luthe_b200 as L
+    import oracle
+    p = L.default_params()
+    k = L.keygen(p, 3)
+    g = torch.Generator(device="cuda").manual_seed(11)
+    with L.Engine(p) as e:
+        e.upload_keys(k)
+        pa = torch.randint(0, 2**62, (4096, 2048), dtype=torch.int64, device="cuda", generator=g)
+        pb = torch.randint(0, 2**62, (4096, 2048), dtype=torch.int64, device="cuda", generator=g)
+        po = torch.empty_like(pa)
+        e.ntt_mul(pa, pb, po, 4096)
+        ks_in = torch.randint(-2**62, 2**62, (16384, 2049), dtype=torch.int64, device="cuda", generator=g)
+        o21 = torch.empty((16384, p.lwe_dim + 1), dtype=torch.int32, device="cuda")
+        o2n = torch.empty_like(o21)
+        e.keyswitch(ks_in, o21, o2n, 16384)
+        torch.cuda.synchronize()
+        e.check_device_error()
+        a4, b4, o4 = (x[:4].cpu().numpy().view(np.uint64) for x in (pa, pb, po))
+        assert np.array_equal(o4, oracle.negacyclic_mul(a4, b4))
+        k4, r4 = ks_in[:4].cpu().numpy().view(np.uint64), o21[:4].cpu().numpy().view(np.uint32)
+        for c in range(4):
+            assert np.array_equal(r4[c], oracle.keyswitch(k4[c], k["ksk"], p.lwe_dim, p.poly_size)[0])
+    print("ncu case other ok")
+
+
 def main():
     args = parse()
     if args.ncu_case:
-        return ncu_case()
+        return ncu_case_other() if args.ncu_case == "other" else ncu_case()
     if args.impl == "reference":
         return reference_arm(args)
     import torch
