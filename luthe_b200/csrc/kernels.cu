@@ -999,6 +999,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
             for (int p = 0; p < 8; p++)
                 rr[p] = gl::mul_add2(x0src[p * TPG + t], hs[(p * 2) * TPG + t], x1src[p * TPG + t],
                                      hs[(p * 2 + 1) * TPG + t]);
+            // split cluster barrier: arrive once this thread's reads of the
+            // other CTA's bp are done, wait only before bp is written again,
+            // so the barrier's latency overlaps the first inverse pass
+            asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
             __syncthreads();  // every read of the half slab is done
             if (t == 0 && i + 1 < n) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1006,7 +1010,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                 issue_half_slab(hs, bsk + (size_t)(i + 1) * SLAB_WORDS, r, mbar);
             }
             ntt::c2_inv(rr, bq, t);
-            cluster.sync();  // the other CTA has finished reading this CTA's bp
+            __syncthreads();  // bq complete (the cluster arrive came before these writes)
+            asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");  // the other CTA has finished reading this CTA's bp
             ntt::c1_inv<1>(bq, bp, t);
             __syncthreads();
             ntt::a2_inv<1>(bp, bq, tws + 2048, t);
