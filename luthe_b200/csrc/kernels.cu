@@ -876,14 +876,20 @@ static size_t br_split_smem_bytes() { return (size_t)(SLAB_WORDS + 4096 + 4 * PO
 
 // Half of a step's BSK slab: column col of both rows, hs[(p*2 + row)*TPG + t]
 // = slab[(p*4 + row*2 + col)*TPG + t] -- sixteen 2 KiB bulk copies.
-__device__ __forceinline__ void issue_half_slab(u64 *hs, const u64 *src, u32 col, u64 *mbar)
+// Called by the 32 lanes of warp 0: lane 0 arms the mbarrier with the byte
+// count, then lanes 0-15 each start one of the 16 pieces of column `col`
+// (2 KiB each), so that no single thread issues sixteen copies in a row
+// while the rest of the CTA waits at the next barrier.  Each issuing lane
+// first orders its earlier shared-memory accesses before the async copies.
+__device__ __forceinline__ void issue_half_slab_warp(u64 *hs, const u64 *src, u32 col, u64 *mbar, int lane)
 {
-    mbar_expect_tx(mbar, (u32)(SLAB_BYTES / 2));
-#pragma unroll
-    for (int p = 0; p < 8; p++)
-#pragma unroll
-        for (int row = 0; row < 2; row++)
-            bulk_g2s(hs + (p * 2 + row) * TPG, src + (p * 4 + row * 2 + col) * TPG, TPG * 8, mbar);
+    if (lane == 0) mbar_expect_tx(mbar, (u32)(SLAB_BYTES / 2));
+    __syncwarp();
+    if (lane < 16) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const int p = lane >> 1, row = lane & 1;
+        bulk_g2s(hs + (p * 2 + row) * TPG, src + (p * 4 + row * 2 + col) * TPG, TPG * 8, mbar);
+    }
 }
 
 // More than half an SM's shared memory, so that the two CTAs of a pair never
@@ -949,10 +955,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
             acc[e] = lut[j];
             bp[j] = acc[e];
         }
-        if (t == 0) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the last reads of hs
-            *last_parity = phase;
-            issue_half_slab(hs, bsk, r, mbar);
+        if (t < 32) {  // warp 0; the last reads of hs were before this ciphertext's barriers
+            if (t == 0) *last_parity = phase;
+            issue_half_slab_warp(hs, bsk, r, mbar, t);
         }
 
         u32 a_next = my_lwe[0];
@@ -1004,10 +1009,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
             // so the barrier's latency overlaps the first inverse pass
             asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
             __syncthreads();  // every read of the half slab is done
-            if (t == 0 && i + 1 < n) {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                *last_parity = phase;
-                issue_half_slab(hs, bsk + (size_t)(i + 1) * SLAB_WORDS, r, mbar);
+            if (t < 32 && i + 1 < n) {  // warp 0
+                if (t == 0) *last_parity = phase;
+                issue_half_slab_warp(hs, bsk + (size_t)(i + 1) * SLAB_WORDS, r, mbar, t);
             }
             ntt::c2_inv(rr, bq, t);
             __syncthreads();  // bq complete (the cluster arrive came before these writes)
