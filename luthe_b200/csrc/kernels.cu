@@ -899,9 +899,10 @@ constexpr size_t PAIR_SMEM_BYTES = 120 * 1024;
 // Lowest-latency form, for batches of at most one ciphertext per two SMs: a
 // cluster of two CTAs (256 threads each, one per SM) per ciphertext, CTA r
 // owning polynomial r -- the split form above with the two groups on two
-// SMs.  Each CTA streams only its half of the slab (column r); around the
-// BSK multiply each reads the other's forward transform through distributed
-// shared memory, between cluster barriers.  A slab timeout is agreed by the
+// SMs.  Each CTA streams only its half of the slab (column r); for the BSK
+// multiply each CTA stores its forward transform into a receive buffer in the
+// other CTA's shared memory as it computes it (remote stores do not stall the
+// writer), and reads only local shared memory after the cluster barrier.  A slab timeout is agreed by the
 // pair through status flags written into both CTAs' shared memory before the
 // first of those barriers, so both leave the step loop at the same point and
 // every cluster barrier is reached by both.
@@ -922,12 +923,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     u64 *mbar = bq + POLY_WORDS;
     u32 *flags = reinterpret_cast<u32 *>(mbar + 1);  // step status of rank 0 and rank 1
     u32 *last_parity = flags + 2;                     // phase parity of the last half slab issued
+    u64 *rx = mbar + 4;  // the other CTA's forward transform, own-slot layout (2048 words)
     const unsigned long long polls = g_slab_wait_polls;
     const u64 tie_rtl = tie_rule == TIE_RTL ? 1ull : 0ull;
     const int t = threadIdx.x;
-    const u64 *peer_bp = cluster.map_shared_rank(bp, r ^ 1u);
+    u64 *peer_rx = cluster.map_shared_rank(rx, r ^ 1u);
     u32 *peer_flags = cluster.map_shared_rank(flags, r ^ 1u);
-    const u64 *x0src = r == 0 ? bp : peer_bp, *x1src = r == 0 ? peer_bp : bp;
+    const u64 *x0src = r == 0 ? bp : rx, *x1src = r == 0 ? rx : bp;
 
     for (int i = t; i < 4096; i += TPG) tws[i] = tw[i];
     if (t == 0) {
@@ -986,7 +988,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                 u64 y[8];
                 ntt::c2_fwd(bq, y, t);
 #pragma unroll
-                for (int p = 0; p < 8; p++) bp[p * TPG + t] = y[p];  // own slots
+                for (int p = 0; p < 8; p++) {
+                    bp[p * TPG + t] = y[p];       // own slots
+                    peer_rx[p * TPG + t] = y[p];  // the other CTA's receive buffer
+                }
             }
             const bool cta_ok = !__syncthreads_or(!mbar_wait(mbar, phase, polls));
             phase ^= 1;
@@ -994,7 +999,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                 flags[r] = cta_ok;
                 peer_flags[r] = cta_ok;
             }
-            cluster.sync();  // both transforms and both status flags are visible
+            cluster.sync();  // both transforms (rx) and both status flags are visible
             if (!(flags[0] && flags[1])) {
                 ok = false;  // same decision in both CTAs
                 break;
@@ -1004,9 +1009,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
             for (int p = 0; p < 8; p++)
                 rr[p] = gl::mul_add2(x0src[p * TPG + t], hs[(p * 2) * TPG + t], x1src[p * TPG + t],
                                      hs[(p * 2 + 1) * TPG + t]);
-            // split cluster barrier: arrive once this thread's reads of the
-            // other CTA's bp are done, wait only before bp is written again,
-            // so the barrier's latency overlaps the first inverse pass
+            // split cluster barrier: arrive once this thread's reads of rx are
+            // done, wait before the next step's stores into the other CTA's rx
+            // (the wait sits before c1_inv, so the barrier's latency overlaps
+            // the first inverse pass)
             asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
             __syncthreads();  // every read of the half slab is done
             if (t < 32 && i + 1 < n) {  // warp 0
@@ -1015,7 +1021,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
             }
             ntt::c2_inv(rr, bq, t);
             __syncthreads();  // bq complete (the cluster arrive came before these writes)
-            asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");  // the other CTA has finished reading this CTA's bp
+            asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");  // the other CTA has finished reading its rx
             ntt::c1_inv<1>(bq, bp, t);
             __syncthreads();
             ntt::a2_inv<1>(bp, bq, tws + 2048, t);
