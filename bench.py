@@ -49,9 +49,10 @@ def parse():
                     help="skip the KS+PBS measurement of the reference's other parameter sets")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shape (profiling runs: no tuning trials among the launches)")
-    ap.add_argument("--ncu-case", nargs="?", const="pbs", choices=("pbs", "other"),
+    ap.add_argument("--ncu-case", nargs="?", const="pbs", choices=("pbs", "other", "plain"),
                     help="small profiling case, then exit: 'pbs' (default) KS+PBS of 296 BLWEs (one persistent "
-                         "wave), twice; 'other' the NTT product of 4096 pairs and the key switch of 16384 BLWEs, once each")
+                         "wave), twice; 'other' the NTT product of 4096 pairs and the key switch of 16384 BLWEs, once "
+                         "each; 'plain' KS+PBS of one BLWE (the 2-SM latency form), twice")
     return ap.parse_args()
 
 
@@ -395,14 +396,14 @@ def config_dict():
     }
 
 
-def ncu_case():
-    """KS+PBS of 296 identity-LUT BLWEs twice (the case the ncu summaries under
-    profiles/ are captured on), checked by decryption."""
+def ncu_case(B=296):
+    """KS+PBS of B identity-LUT BLWEs twice (296: one persistent wave, the case
+    the blind-rotation ncu summaries under profiles/ are captured on; 1: the
+    plain path), checked by decryption."""
     import torch
     import luthe_b200 as L
     p = L.default_params()
     k = L.keygen(p, 3)
-    B = 296
     with L.Engine(p) as e:
         e.upload_keys(k)
         e.upload_luts(L.lut_build(p, np.arange(16, dtype=np.uint32)))
@@ -452,7 +453,9 @@ def ncu_case_other():
 def main():
     args = parse()
     if args.ncu_case:
-        return ncu_case_other() if args.ncu_case == "other" else ncu_case()
+        if args.ncu_case == "other":
+            return ncu_case_other()
+        return ncu_case(1 if args.ncu_case == "plain" else 296)
     if args.impl == "reference":
         return reference_arm(args)
     import torch
