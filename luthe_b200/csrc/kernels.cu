@@ -894,7 +894,7 @@ __device__ __forceinline__ void issue_half_slab_warp(u64 *hs, const u64 *src, u3
 
 // More than half an SM's shared memory, so that the two CTAs of a pair never
 // share an SM.
-constexpr size_t PAIR_SMEM_BYTES = 120 * 1024;
+constexpr size_t PAIR_SMEM_BYTES = 132 * 1024;
 
 // Lowest-latency form, for batches of at most one ciphertext per two SMs: a
 // cluster of two CTAs (256 threads each, one per SM) per ciphertext, CTA r
@@ -902,7 +902,10 @@ constexpr size_t PAIR_SMEM_BYTES = 120 * 1024;
 // SMs.  Each CTA streams only its half of the slab (column r); for the BSK
 // multiply each CTA stores its forward transform into a receive buffer in the
 // other CTA's shared memory as it computes it (remote stores do not stall the
-// writer), and reads only local shared memory after the cluster barrier.  A slab timeout is agreed by the
+// writer), and reads only local shared memory after the cluster barrier.
+// The receive buffers and the status flags alternate by step parity, so a
+// buffer is written again only two steps later, after the next step's
+// cluster barrier has ordered this step's reads: one cluster barrier a step.  A slab timeout is agreed by the
 // pair through status flags written into both CTAs' shared memory before the
 // first of those barriers, so both leave the step loop at the same point and
 // every cluster barrier is reached by both.
@@ -921,15 +924,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     u64 *tws = hs + SLAB_WORDS / 2;
     u64 *bp = tws + 4096, *bq = bp + POLY_WORDS;
     u64 *mbar = bq + POLY_WORDS;
-    u32 *flags = reinterpret_cast<u32 *>(mbar + 1);  // step status of rank 0 and rank 1
-    u32 *last_parity = flags + 2;                     // phase parity of the last half slab issued
-    u64 *rx = mbar + 4;  // the other CTA's forward transform, own-slot layout (2048 words)
+    u32 *flags = reinterpret_cast<u32 *>(mbar + 1);  // [step parity][rank]: step status of rank 0 and rank 1
+    u32 *last_parity = flags + 4;                     // phase parity of the last half slab issued
+    u64 *rx = mbar + 4;  // [step parity][2048]: the other CTA's forward transform, own-slot layout
     const unsigned long long polls = g_slab_wait_polls;
     const u64 tie_rtl = tie_rule == TIE_RTL ? 1ull : 0ull;
     const int t = threadIdx.x;
     u64 *peer_rx = cluster.map_shared_rank(rx, r ^ 1u);
     u32 *peer_flags = cluster.map_shared_rank(flags, r ^ 1u);
-    const u64 *x0src = r == 0 ? bp : rx, *x1src = r == 0 ? rx : bp;
+    u32 step = 0;  // steps run by this CTA, over all its ciphertexts: the parity of rx and flags
 
     for (int i = t; i < 4096; i += TPG) tws[i] = tw[i];
     if (t == 0) {
@@ -989,39 +992,37 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                 ntt::c2_fwd(bq, y, t);
 #pragma unroll
                 for (int p = 0; p < 8; p++) {
-                    bp[p * TPG + t] = y[p];       // own slots
-                    peer_rx[p * TPG + t] = y[p];  // the other CTA's receive buffer
+                    bp[p * TPG + t] = y[p];                           // own slots
+                    peer_rx[(step & 1) * N + p * TPG + t] = y[p];  // the other CTA's receive buffer
                 }
             }
             const bool cta_ok = !__syncthreads_or(!mbar_wait(mbar, phase, polls));
             phase ^= 1;
+            u32 *fl = flags + 2 * (step & 1);
             if (t == 0) {
-                flags[r] = cta_ok;
-                peer_flags[r] = cta_ok;
+                fl[r] = cta_ok;
+                peer_flags[2 * (step & 1) + r] = cta_ok;
             }
             cluster.sync();  // both transforms (rx) and both status flags are visible
-            if (!(flags[0] && flags[1])) {
+            if (!(fl[0] && fl[1])) {
                 ok = false;  // same decision in both CTAs
                 break;
             }
+            const u64 *rxs = rx + (step & 1) * N;
+            const u64 *x0src = r == 0 ? bp : rxs, *x1src = r == 0 ? rxs : bp;
+            step++;
             u64 rr[8];
 #pragma unroll
             for (int p = 0; p < 8; p++)
                 rr[p] = gl::mul_add2(x0src[p * TPG + t], hs[(p * 2) * TPG + t], x1src[p * TPG + t],
                                      hs[(p * 2 + 1) * TPG + t]);
-            // split cluster barrier: arrive once this thread's reads of rx are
-            // done, wait before the next step's stores into the other CTA's rx
-            // (the wait sits before c1_inv, so the barrier's latency overlaps
-            // the first inverse pass)
-            asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
             __syncthreads();  // every read of the half slab is done
             if (t < 32 && i + 1 < n) {  // warp 0
                 if (t == 0) *last_parity = phase;
                 issue_half_slab_warp(hs, bsk + (size_t)(i + 1) * SLAB_WORDS, r, mbar, t);
             }
             ntt::c2_inv(rr, bq, t);
-            __syncthreads();  // bq complete (the cluster arrive came before these writes)
-            asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");  // the other CTA has finished reading its rx
+            __syncthreads();
             ntt::c1_inv<1>(bq, bp, t);
             __syncthreads();
             ntt::a2_inv<1>(bp, bq, tws + 2048, t);
