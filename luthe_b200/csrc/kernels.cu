@@ -905,10 +905,11 @@ constexpr size_t PAIR_SMEM_BYTES = 132 * 1024;
 // writer), and reads only local shared memory after the cluster barrier.
 // The receive buffers and the status flags alternate by step parity, so a
 // buffer is written again only two steps later, after the next step's
-// cluster barrier has ordered this step's reads: one cluster barrier a step.  A slab timeout is agreed by the
-// pair through status flags written into both CTAs' shared memory before the
-// first of those barriers, so both leave the step loop at the same point and
-// every cluster barrier is reached by both.
+// cluster barrier has ordered this step's reads: one cluster barrier a step.
+// A slab timeout is agreed by the pair through those status flags, written
+// into both CTAs' shared memory before the step's cluster barrier, so both
+// leave the step loop at the same point and every cluster barrier is reached
+// by both.
 template <int BW>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     br_kernel_pair(const u32 *__restrict__ lwe2N, const u64 *__restrict__ luts, const u32 *__restrict__ lut_id,
