@@ -140,6 +140,8 @@ extern "C" void luthe_ctx_destroy(luthe_ctx *c)
     dfree(c, c->d_hin, c->hcap * (N + 1) * 8);
     dfree(c, c->d_hout, c->hcap * (N + 1) * 8);
     dfree(c, c->d_hids, c->hcap * 4);
+    if (c->ev_main) cudaEventDestroy(c->ev_main);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     delete c;
 }
 
@@ -369,12 +371,33 @@ extern "C" int luthe_ks_pbs_host(luthe_ctx *c, const uint64_t *h_in, const uint3
         c->hcap = count;
     }
     if ((r = ensure_scratch(c, count))) return r;
+    if (!c->copy_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming));
+    }
     cudaStream_t s = 0;
-    CUDA_TRY(cudaMemcpyAsync(c->d_hin, h_in, count * (N + 1) * 8, cudaMemcpyHostToDevice, s));
+    const uint32_t n = c->p.lwe_dim;
+    const size_t row = (size_t)(N + 1);
+    CUDA_TRY(cudaMemcpyAsync(c->d_hin, h_in, count * row * 8, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(c->d_hids, h_ids, count * 4, cudaMemcpyHostToDevice, s));
-    if ((r = enqueue_ks_pbs(c, c->d_hin, c->d_hids, c->d_hout, count, s))) return r;
-    CUDA_TRY(cudaMemcpyAsync(h_out, c->d_hout, count * (N + 1) * 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(launch_keyswitch(c->d_hin, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr,
+                              c->p.ks_base_log, c->p.ks_level, c->tie_rule, c->d_ks_part));
+    size_t full = count;
+    CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, c->d_hids, c->nlut, c->d_bsk, c->d_tw,
+                                 c->d_hout, count, n, c->d_err, s, nullptr, 1, c->p.pbs_base_log, c->tie_rule,
+                                 c->ev_main, &full));
+    size_t early = 0;  // outputs read back on the copy stream while the tail launch runs
+    if (full < count) {
+        // the full waves' outputs are final before the tail launch: their
+        // read-back overlaps the tail on the copy stream
+        early = full;
+        CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, c->ev_main, 0));
+        CUDA_TRY(cudaMemcpyAsync(h_out, c->d_hout, early * row * 8, cudaMemcpyDeviceToHost, c->copy_stream));
+    }
+    CUDA_TRY(cudaMemcpyAsync(h_out + early * row, c->d_hout + early * row, (count - early) * row * 8,
+                             cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
     return luthe_check_device_error(c);
 }
 

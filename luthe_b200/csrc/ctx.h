@@ -34,6 +34,8 @@ struct luthe_ctx {
     uint64_t *d_hin = nullptr, *d_hout = nullptr;
     uint32_t *d_hids = nullptr;
     size_t hcap = 0;
+    cudaStream_t copy_stream = nullptr;  // host path: read-back of the full waves while the tail runs
+    cudaEvent_t ev_main = nullptr;       // recorded after the full waves' launch
     luthe::BrConfig br{2, 1};
     uint32_t tie_rule = luthe::TIE_RTL;  // decomposition tie rule (luthe_set_tie_rule)
     std::vector<GraphEntry> graphs;

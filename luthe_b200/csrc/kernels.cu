@@ -1154,8 +1154,14 @@ static cudaError_t launch_br_once(int G, int ctas_per_sm, int nsm, const uint32_
 cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_lwe2N, const uint64_t *d_luts,
                                 const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
                                 uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s,
-                                const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw, uint32_t tie_rule)
+                                const uint32_t *d_dst_idx, uint32_t mlk, uint32_t pbs_bw, uint32_t tie_rule,
+                                cudaEvent_t main_done, size_t *main_count)
 {
+    // main_count (optional) receives the number of leading ciphertexts whose
+    // outputs are final once main_done (optional) fires on s: the full waves
+    // when a tail launch follows them (the event is then recorded between the
+    // two launches), else the whole batch (no event is recorded).
+    if (main_count) *main_count = B;
     if (B == 0) return cudaSuccess;
     if (mlk != 1 && mlk != 2 && mlk != 4 && mlk != 8) return cudaErrorInvalidValue;
     if (!pbs_supported(pbs_bw)) return cudaErrorInvalidValue;
@@ -1182,6 +1188,8 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int nsm, const uint32_t *d_
         cudaError_t e = launch_br_once(G, cps, nsm, d_lwe2N, d_luts, d_lut_id, nlut, d_bsk, d_tw, d_out, full, n,
                                        d_err, s, d_dst_idx, mlk, pbs_bw, tie_rule);
         if (e != cudaSuccess) return e;
+        if (main_done && (e = cudaEventRecord(main_done, s)) != cudaSuccess) return e;
+        if (main_count) *main_count = full;
         uint64_t *out_tail = d_dst_idx ? d_out : d_out + full * mlk * (size_t)(N + 1);
         return launch_br_once(small_form(tail), 1, nsm, d_lwe2N + full * (size_t)(n + 1), d_luts, d_lut_id + full,
                               nlut, d_bsk, d_tw, out_tail, tail, n, d_err, s, d_dst_idx ? d_dst_idx + full : nullptr,

@@ -58,7 +58,8 @@ cudaError_t launch_blind_rotate(const BrConfig &cfg, int num_sms, const uint32_t
                                 const uint32_t *d_lut_id, uint32_t nlut, const uint64_t *d_bsk, const uint64_t *d_tw,
                                 uint64_t *d_out, size_t B, uint32_t n, uint32_t *d_err, cudaStream_t s,
                                 const uint32_t *d_dst_idx = nullptr, uint32_t mlk = 1, uint32_t pbs_bw = 23,
-                                uint32_t tie_rule = TIE_RTL);
+                                uint32_t tie_rule = TIE_RTL, cudaEvent_t main_done = nullptr,
+                                size_t *main_count = nullptr);
 size_t br_smem_bytes(const BrConfig &cfg, uint32_t n);
 cudaError_t br_set_attributes(const BrConfig &cfg, uint32_t n);
 

@@ -64,7 +64,8 @@ cudaError_t launch_keyswitch(const uint64_t *in, const uint32_t *, uint32_t *, u
 }
 cudaError_t launch_blind_rotate(const BrConfig &, int, const uint32_t *l2n, const uint64_t *luts, const uint32_t *ids,
                                 uint32_t, const uint64_t *, const uint64_t *, uint64_t *out, size_t B, uint32_t n,
-                                uint32_t *, cudaStream_t, const uint32_t *dst_idx, uint32_t mlk, uint32_t, uint32_t)
+                                uint32_t *, cudaStream_t, const uint32_t *dst_idx, uint32_t mlk, uint32_t, uint32_t,
+                                cudaEvent_t, size_t *)
 {
     for (size_t c = 0; c < B; c++) {
         const uint32_t x = l2n[c * (n + 1)];

@@ -82,3 +82,28 @@ def test_largest_batch_in_one_call(engine, params, keys, oracle_bsk):
     sel = np.unique(np.r_[0:8, count - 8:count, rng.choice(count, 24, replace=False)])
     want = oracle_bsk.ks_pbs(keys["ksk"], ct[sel], luts, ids[sel])
     assert np.array_equal(got[sel], want)
+
+
+def test_host_entry_point_with_a_tail_launch(engine, params, keys, oracle_bsk):
+    """A batch of full waves plus a tail (one wave of 296 on 148 SMs + 7),
+    through luthe_ks_pbs_host, whose read-back of the full waves overlaps the
+    tail launch: equal to the device entry point and, on a sample, to the
+    oracle, on two calls in a row."""
+    count = 303
+    rng = np.random.default_rng(303)
+    tables = [rng.integers(0, 16, 16).astype(np.uint32) for _ in range(3)]
+    luts = np.stack([L.lut_build(params, t) for t in tables])
+    msgs = rng.integers(0, 16, count).astype(np.uint32)
+    ids = rng.integers(0, 3, count).astype(np.uint32)
+    ct = L.encrypt(params, keys["glwe_key"], msgs, 303)
+    engine.upload_luts(luts)
+    engine.set_br_config(2, 1)
+    d_out = to_dev(np.zeros_like(ct))
+    engine.ks_pbs(to_dev(ct), to_dev(ids), d_out, count)
+    engine.check_device_error()
+    want_dev = from_dev(d_out, np.uint64)
+    for _ in range(2):
+        got = engine.ks_pbs_host(ct, ids)
+        assert np.array_equal(got, want_dev)
+    sel = np.r_[0:4, count - 12:count]
+    assert np.array_equal(want_dev[sel], oracle_bsk.ks_pbs(keys["ksk"], ct[sel], luts, ids[sel]))
