@@ -134,9 +134,12 @@ int luthe_reserve(luthe_ctx *ctx, size_t max_count);
 int luthe_ks_pbs(luthe_ctx *ctx, const uint64_t *d_in, const uint32_t *d_lut_id, uint64_t *d_out, size_t count,
                  void *stream);
 /* Same through host buffers (copies in, computes, copies out, synchronises).
- * Pinned host memory gives the full PCIe/C2C bandwidth.  When the batch ends
- * in a partial wave that runs as its own launch, the outputs of the full
- * waves are copied back on a stream of the context while that launch runs. */
+ * Pinned host memory gives the full PCIe/C2C bandwidth.  Batches of 1024 or
+ * more are copied in as two chunks (a quarter, then the rest) on a stream of
+ * the context, each chunk's key switch starting once it has landed; when the
+ * batch ends in a partial
+ * wave that runs as its own launch, the outputs of the full waves are copied
+ * back on that stream while that launch runs. */
 int luthe_ks_pbs_host(luthe_ctx *ctx, const uint64_t *h_in, const uint32_t *h_lut_id, uint64_t *h_out,
                       size_t count);
 /* Many-LUT PBS (PBS_ML2/ML4/ML8, docs/dop.md:101-121): one blind rotation per

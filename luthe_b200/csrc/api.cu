@@ -141,6 +141,7 @@ extern "C" void luthe_ctx_destroy(luthe_ctx *c)
     dfree(c, c->d_hout, c->hcap * (N + 1) * 8);
     dfree(c, c->d_hids, c->hcap * 4);
     if (c->ev_main) cudaEventDestroy(c->ev_main);
+    if (c->ev_in) cudaEventDestroy(c->ev_in);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     delete c;
 }
@@ -374,14 +375,27 @@ extern "C" int luthe_ks_pbs_host(luthe_ctx *c, const uint64_t *h_in, const uint3
     if (!c->copy_stream) {
         CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
     }
     cudaStream_t s = 0;
     const uint32_t n = c->p.lwe_dim;
     const size_t row = (size_t)(N + 1);
-    CUDA_TRY(cudaMemcpyAsync(c->d_hin, h_in, count * row * 8, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(c->d_hids, h_ids, count * 4, cudaMemcpyHostToDevice, s));
-    CUDA_TRY(launch_keyswitch(c->d_hin, c->d_ksk, nullptr, c->d_lwe2N, count, n, c->xpad, s, nullptr,
-                              c->p.ks_base_log, c->p.ks_level, c->tie_rule, c->d_ks_part));
+    // inputs in two chunks on the copy stream, each chunk's key switch as soon
+    // as it has landed: a quarter first, whose copy is the only one not hidden
+    // behind compute, then the rest, whose key switch still fills the GPU
+    const size_t first = count >= 1024 ? (count / 4 + KS_BM - 1) / KS_BM * KS_BM : count;
+    for (int k = 0; k < 2; k++) {
+        const size_t off = k ? first : 0, m = (k ? count : first) - off;
+        if (m == 0) continue;
+        CUDA_TRY(cudaMemcpyAsync(c->d_hin + off * row, h_in + off * row, m * row * 8, cudaMemcpyHostToDevice,
+                                 c->copy_stream));
+        CUDA_TRY(cudaEventRecord(c->ev_in, c->copy_stream));
+        CUDA_TRY(cudaStreamWaitEvent(s, c->ev_in, 0));
+        CUDA_TRY(launch_keyswitch(c->d_hin + off * row, c->d_ksk, nullptr, c->d_lwe2N + off * (size_t)(n + 1), m,
+                                  n, c->xpad, s, nullptr, c->p.ks_base_log, c->p.ks_level, c->tie_rule,
+                                  c->d_ks_part));
+    }
     size_t full = count;
     CUDA_TRY(launch_blind_rotate(c->br, c->nsm, c->d_lwe2N, c->d_luts, c->d_hids, c->nlut, c->d_bsk, c->d_tw,
                                  c->d_hout, count, n, c->d_err, s, nullptr, 1, c->p.pbs_base_log, c->tie_rule,

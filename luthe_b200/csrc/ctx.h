@@ -36,6 +36,7 @@ struct luthe_ctx {
     size_t hcap = 0;
     cudaStream_t copy_stream = nullptr;  // host path: read-back of the full waves while the tail runs
     cudaEvent_t ev_main = nullptr;       // recorded after the full waves' launch
+    cudaEvent_t ev_in = nullptr;         // host path: a chunk of inputs has landed
     luthe::BrConfig br{2, 1};
     uint32_t tie_rule = luthe::TIE_RTL;  // decomposition tie rule (luthe_set_tie_rule)
     std::vector<GraphEntry> graphs;

@@ -84,18 +84,19 @@ def test_largest_batch_in_one_call(engine, params, keys, oracle_bsk):
     assert np.array_equal(got[sel], want)
 
 
-def test_host_entry_point_with_a_tail_launch(engine, params, keys, oracle_bsk):
-    """A batch of full waves plus a tail (one wave of 296 on 148 SMs + 7),
+@pytest.mark.parametrize("count", [303, 1191])
+def test_host_entry_point_with_a_tail_launch(engine, params, keys, oracle_bsk, count):
+    """Batches of full waves plus a tail (1 and 4 waves of 296 on 148 SMs, + 7)
     through luthe_ks_pbs_host, whose read-back of the full waves overlaps the
-    tail launch: equal to the device entry point and, on a sample, to the
-    oracle, on two calls in a row."""
-    count = 303
-    rng = np.random.default_rng(303)
+    tail launch (1191 also copies its inputs in two chunks under the key
+    switch): equal to the device entry point and, on a sample, to the oracle,
+    on two calls in a row."""
+    rng = np.random.default_rng(count)
     tables = [rng.integers(0, 16, 16).astype(np.uint32) for _ in range(3)]
     luts = np.stack([L.lut_build(params, t) for t in tables])
     msgs = rng.integers(0, 16, count).astype(np.uint32)
     ids = rng.integers(0, 3, count).astype(np.uint32)
-    ct = L.encrypt(params, keys["glwe_key"], msgs, 303)
+    ct = L.encrypt(params, keys["glwe_key"], msgs, count)
     engine.upload_luts(luts)
     engine.set_br_config(2, 1)
     d_out = to_dev(np.zeros_like(ct))
