@@ -133,7 +133,7 @@ extern "C" void luthe_ctx_destroy(luthe_ctx *c)
     dfree(c, c->d_tw, 4096 * 8);
     dfree(c, c->d_err, 4);
     dfree(c, c->d_bsk, n * SLAB_BYTES);
-    dfree(c, c->d_ksk, (size_t)N * c->p.ks_level * c->xpad * 4);
+    dfree(c, c->d_ksk, (size_t)N * c->p.ks_level / 4 * KS_PLANES * c->xpad * 4);
     dfree(c, c->d_ks_part, (size_t)KS_BM * c->xpad * 4);
     dfree(c, c->d_luts, (size_t)c->nlut * 2 * N * 8);
     dfree(c, c->d_lwe2N, c->cap * (n + 1) * 4);
@@ -211,18 +211,24 @@ extern "C" int luthe_upload_ksk(luthe_ctx *c, const uint32_t *h)
     CUDA_TRY(cudaSetDevice(c->device));
     const size_t n = c->p.lwe_dim, K = (size_t)N * c->p.ks_level;
     const uint32_t xpad = (uint32_t)(((n + 1) + KS_BN - 1) / KS_BN * KS_BN);
-    std::vector<uint32_t> t((size_t)K * xpad, 0);
+    // device layout [K/4][byte plane][xpad]: byte b of rows 4g..4g+3 in one word
+    const size_t words = K / 4 * KS_PLANES * xpad;
+    std::vector<uint32_t> t(words, 0);
     const uint32_t M = (1u << KS_W) - 1;
     for (size_t x = 0; x <= n; x++)
-        for (size_t k = 0; k < K; k++) t[k * xpad + x] = h[x * K + k] & M;
+        for (size_t k = 0; k < K; k++) {
+            const uint32_t v = h[x * K + k] & M;
+            for (int b = 0; b < KS_PLANES; b++)
+                t[((k / 4) * KS_PLANES + b) * xpad + x] |= ((v >> (8 * b)) & 0xFFu) << (8 * (k % 4));
+        }
     int r;
     if (!c->d_ksk) {
-        if ((r = dalloc(c, (void **)&c->d_ksk, K * xpad * 4))) return r;
+        if ((r = dalloc(c, (void **)&c->d_ksk, words * 4))) return r;
         c->xpad = xpad;
         if ((r = dalloc(c, (void **)&c->d_ks_part, (size_t)KS_BM * xpad * 4))) return r;
         CUDA_TRY(cudaMemset(c->d_ks_part, 0, (size_t)KS_BM * xpad * 4));
     }
-    CUDA_TRY(cudaMemcpy(c->d_ksk, t.data(), K * xpad * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(c->d_ksk, t.data(), words * 4, cudaMemcpyHostToDevice));
     return LUTHE_OK;
 }
 

@@ -235,7 +235,10 @@ cudaError_t launch_ntt_mul(const uint64_t *d_a, const uint64_t *d_b, uint64_t *d
 //  pep_ks_out_process.sv:276-280,336-341).  A SIMT integer GEMM: M = ciphertexts,
 // N = output coefficients, K = (y, z) pairs.  The digits (in [-4, 4]) are made
 // on the fly from the 64-bit mask coefficients; 32-bit wrap-around keeps the
-// low 21 bits exact.  KSK is transposed to [y*L+z][x] on upload.  Templated
+// low 21 bits exact.  On upload the KSK is transposed to K-rows k = y*L+z and
+// split into byte planes: word [k/4][b][x] holds byte b of KSK[k..k+3][x], so
+// one dp4a multiplies four rows' bytes by four packed digits (signed bytes)
+// and three dp4a replace four 32-bit multiply-adds.  Templated
 // on the decomposition (base 2^BL, L levels) of the reference's parameter sets.
 // GEN = false: the RTL's tie rule; GEN = true: the rule of the reference's
 // test-vector generator (TFHE-rs), which takes the digit above the top one as
@@ -263,22 +266,35 @@ __device__ __forceinline__ void ks_decomp(u64 v, int *d)
     }
 }
 
+// acc + sum over the 4 bytes of (unsigned byte of k) * (signed byte of d)
+__device__ __forceinline__ int dp4a_us(u32 k, u32 d, int acc)
+{
+    int r;
+    asm("dp4a.u32.s32 %0, %1, %2, %3;" : "=r"(r) : "r"(k), "r"(d), "r"(acc));
+    return r;
+}
+
 template <int BL, int L, bool GEN>
 __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, const u32 *__restrict__ src_idx,
                                                   const u32 *__restrict__ ksk_t, u32 *__restrict__ out21,
                                                   u32 *__restrict__ out2N, u32 B, u32 n, u32 xpad,
                                                   u32 *__restrict__ part)
 {
-    __shared__ __align__(16) int dsm[KS_KC * L][KS_BM];  // digits [k][ct]
-    __shared__ __align__(16) u32 ksm[KS_KC * L][KS_BN];  // KSK tile [k][x]
+    constexpr int KR = KS_KC * L;   // K rows of one chunk (a multiple of 4)
+    constexpr int KG = KR / 4;      // 4-row groups of one chunk
+    __shared__ __align__(16) unsigned char dsm[KS_BM][KR];     // digits, one signed byte each, [ct][k]
+    __shared__ __align__(16) u32 ksm[KG][KS_PLANES][KS_BN];    // KSK bytes, 4 rows per word, [group][plane][x]
     const int tid = threadIdx.x;
     const int ty = tid >> 5, tx = tid & 31;  // 8 x 4 cts, 32 x 4 outputs
     const u32 c0 = blockIdx.y * KS_BM, x0 = blockIdx.x * KS_BN;
-    u32 acc[4][4];
+    // one accumulator per byte plane of the KSK word: KSK = p0 + p1 2^8 + p2 2^16
+    int acc[KS_PLANES][4][4];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int b = 0; b < KS_PLANES; b++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = 0;
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[b][i][j] = 0;
 
     const int dct = tid >> 3, dy = tid & 7;  // decomposition role: 32 cts x 8 coefs
     const u32 dct_c = min(c0 + dct, B - 1);
@@ -291,29 +307,38 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
             int d[L];
             ks_decomp<BL, L, GEN>(in[(size_t)dct_g * (N + 1) + y0 + dy], d);
 #pragma unroll
-            for (int z = 0; z < L; z++) dsm[dy * L + z][dct] = d[z];
+            for (int z = 0; z < L; z++) dsm[dct][dy * L + z] = (unsigned char)(signed char)d[z];
         }
-        const uint4 *src = reinterpret_cast<const uint4 *>(ksk_t + (size_t)y0 * L * xpad + x0);
-#pragma unroll
-        for (int r = 0; r < (KS_KC * L * KS_BN / 4) / 256; r++) {
-            int idx = tid + r * 256;
-            int k = idx / (KS_BN / 4), xv = idx % (KS_BN / 4);
-            reinterpret_cast<uint4 *>(&ksm[k][0])[xv] = src[(size_t)k * (xpad / 4) + xv];
+        // the chunk's KSK rows y0 L .. y0 L + KR - 1 are groups y0 L / 4 ..
+        const uint4 *src = reinterpret_cast<const uint4 *>(ksk_t + (size_t)(y0 * L / 4) * KS_PLANES * xpad + x0);
+        for (int idx = tid; idx < KG * KS_PLANES * (KS_BN / 4); idx += 256) {
+            const int row = idx / (KS_BN / 4), xv = idx % (KS_BN / 4);  // row = group * planes + plane
+            reinterpret_cast<uint4 *>(&ksm[0][0][0] + row * KS_BN)[xv] = src[(size_t)row * (xpad / 4) + xv];
         }
         __syncthreads();
-#pragma unroll 8
-        for (int k = 0; k < KS_KC * L; k++) {
-            int4 dv = reinterpret_cast<const int4 *>(&dsm[k][0])[ty];
-            uint4 kv = reinterpret_cast<const uint4 *>(&ksm[k][0])[tx];
-            int dd[4] = {dv.x, dv.y, dv.z, dv.w};
-            u32 kk[4] = {kv.x, kv.y, kv.z, kv.w};
+#pragma unroll 4
+        for (int g = 0; g < KG; g++) {
+            u32 dv[4];
 #pragma unroll
-            for (int i = 0; i < 4; i++)
+            for (int i = 0; i < 4; i++) dv[i] = *reinterpret_cast<const u32 *>(&dsm[ty * 4 + i][4 * g]);
 #pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] += (u32)dd[i] * kk[j];
+            for (int b = 0; b < KS_PLANES; b++) {
+                const uint4 kv = reinterpret_cast<const uint4 *>(&ksm[g][b][0])[tx];
+                const u32 kk[4] = {kv.x, kv.y, kv.z, kv.w};
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) acc[b][i][j] = dp4a_us(kk[j], dv[i], acc[b][i][j]);
+            }
         }
         __syncthreads();
     }
+    u32 sum[4][4];  // sum_{k} d_k KSK_k mod 2^32 (exact mod 2^21)
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            sum[i][j] = (u32)acc[0][i][j] + ((u32)acc[1][i][j] << 8) + ((u32)acc[2][i][j] << 16);
     if (part) {
         // 32-bit wrap-around sums are exact mod 2^21 in any order
 #pragma unroll
@@ -323,7 +348,7 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const u32 x = x0 + tx * 4 + j;
-                if (x <= n) atomicAdd(&part[(size_t)c * xpad + x], acc[i][j]);
+                if (x <= n) atomicAdd(&part[(size_t)c * xpad + x], sum[i][j]);
             }
         }
         return;
@@ -339,7 +364,7 @@ __global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, con
         for (int j = 0; j < 4; j++) {
             u32 x = x0 + tx * 4 + j;
             if (x > n) continue;
-            u32 v = (((x == n) ? b21 : 0u) - acc[i][j]) & M;
+            u32 v = (((x == n) ? b21 : 0u) - sum[i][j]) & M;
             if (out21) out21[(size_t)c * (n + 1) + x] = v;
             out2N[(size_t)c * (n + 1) + x] = ((v >> 9) + ((v >> 8) & 1u)) & (TWO_N - 1);
         }
