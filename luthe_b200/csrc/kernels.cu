@@ -274,8 +274,11 @@ __device__ __forceinline__ int dp4a_us(u32 k, u32 d, int acc)
     return r;
 }
 
+// three CTAs per SM (80 registers): the multiply pipe needs the warps to hide
+// the dp4a latency (two CTAs per SM at 110 registers: 12.28 ms for 16384 BLWEs,
+// three: 11.49 ms)
 template <int BL, int L, bool GEN>
-__global__ void __launch_bounds__(256) ks_kernel(const u64 *__restrict__ in, const u32 *__restrict__ src_idx,
+__global__ void __launch_bounds__(256, 3) ks_kernel(const u64 *__restrict__ in, const u32 *__restrict__ src_idx,
                                                   const u32 *__restrict__ ksk_t, u32 *__restrict__ out21,
                                                   u32 *__restrict__ out2N, u32 B, u32 n, u32 xpad,
                                                   u32 *__restrict__ part)
