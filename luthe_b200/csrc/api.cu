@@ -211,15 +211,18 @@ extern "C" int luthe_upload_ksk(luthe_ctx *c, const uint32_t *h)
     CUDA_TRY(cudaSetDevice(c->device));
     const size_t n = c->p.lwe_dim, K = (size_t)N * c->p.ks_level;
     const uint32_t xpad = (uint32_t)(((n + 1) + KS_BN - 1) / KS_BN * KS_BN);
-    // device layout [K/4][byte plane][xpad]: byte b of rows 4g..4g+3 in one word
+    // device layout [K/4][3][xpad] for the group g = k/4 of four rows: word 0
+    // the low bytes of rows 4g..4g+3, words 1 and 2 their upper 13 bits as
+    // 16-bit halves (rows 4g, 4g+1 and 4g+2, 4g+3)
     const size_t words = K / 4 * KS_PLANES * xpad;
     std::vector<uint32_t> t(words, 0);
     const uint32_t M = (1u << KS_W) - 1;
     for (size_t x = 0; x <= n; x++)
         for (size_t k = 0; k < K; k++) {
-            const uint32_t v = h[x * K + k] & M;
-            for (int b = 0; b < KS_PLANES; b++)
-                t[((k / 4) * KS_PLANES + b) * xpad + x] |= ((v >> (8 * b)) & 0xFFu) << (8 * (k % 4));
+            const uint32_t v = h[x * K + k] & M, r = (uint32_t)(k % 4);
+            const size_t g = (k / 4) * KS_PLANES;
+            t[g * xpad + x] |= (v & 0xFFu) << (8 * r);
+            t[(g + 1 + r / 2) * xpad + x] |= (v >> 8) << (16 * (r % 2));
         }
     int r;
     if (!c->d_ksk) {

@@ -21,7 +21,7 @@ struct luthe_ctx {
     uint64_t budget = 0, used = 0;
     uint64_t *d_tw = nullptr;     // [2][8][256]
     uint64_t *d_bsk = nullptr;    // [n][8][2][2][256]
-    uint32_t *d_ksk = nullptr;    // [kN*L/4][KS_PLANES][xpad]: byte planes of 4 K-rows per word
+    uint32_t *d_ksk = nullptr;    // [kN*L/4][KS_PLANES][xpad]: 4 K-rows per group (low bytes, upper halves)
     uint32_t xpad = 0;
     uint32_t *d_ks_part = nullptr;  // [KS_BM][xpad] split-K partial sums of small key switches (kept zero)
     uint64_t *d_luts = nullptr;   // [nlut][2][N]

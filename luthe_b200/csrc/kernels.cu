@@ -236,9 +236,12 @@ cudaError_t launch_ntt_mul(const uint64_t *d_a, const uint64_t *d_b, uint64_t *d
 // N = output coefficients, K = (y, z) pairs.  The digits (in [-4, 4]) are made
 // on the fly from the 64-bit mask coefficients; 32-bit wrap-around keeps the
 // low 21 bits exact.  On upload the KSK is transposed to K-rows k = y*L+z and
-// split into byte planes: word [k/4][b][x] holds byte b of KSK[k..k+3][x], so
-// one dp4a multiplies four rows' bytes by four packed digits (signed bytes)
-// and three dp4a replace four 32-bit multiply-adds.  Templated
+// split by groups of four rows g: word [g][0][x] holds the low bytes of rows
+// 4g..4g+3, words [g][1][x] and [g][2][x] their upper 13 bits as 16-bit
+// halves (rows 4g, 4g+1 and 4g+2, 4g+3).  One dp4a multiplies the four low
+// bytes by four packed digits (signed bytes) and two dp2a the upper parts:
+// three instructions replace four 32-bit multiply-adds, with two
+// accumulators per output.  Templated
 // on the decomposition (base 2^BL, L levels) of the reference's parameter sets.
 // GEN = false: the RTL's tie rule; GEN = true: the rule of the reference's
 // test-vector generator (TFHE-rs), which takes the digit above the top one as
@@ -273,10 +276,18 @@ __device__ __forceinline__ int dp4a_us(u32 k, u32 d, int acc)
     asm("dp4a.u32.s32 %0, %1, %2, %3;" : "=r"(r) : "r"(k), "r"(d), "r"(acc));
     return r;
 }
+// acc + (unsigned halves of k) . (signed bytes 0, 1 of d)   [HI: bytes 2, 3]
+template <bool HI>
+__device__ __forceinline__ int dp2a_us(u32 k, u32 d, int acc)
+{
+    int r;
+    if constexpr (HI) asm("dp2a.hi.u32.s32 %0, %1, %2, %3;" : "=r"(r) : "r"(k), "r"(d), "r"(acc));
+    else asm("dp2a.lo.u32.s32 %0, %1, %2, %3;" : "=r"(r) : "r"(k), "r"(d), "r"(acc));
+    return r;
+}
 
-// three CTAs per SM (80 registers): the multiply pipe needs the warps to hide
-// the dp4a latency (two CTAs per SM at 110 registers: 12.28 ms for 16384 BLWEs,
-// three: 11.49 ms)
+// three CTAs per SM (80 registers, no spills with two accumulators per
+// output): the multiply pipe needs the warps to hide the dp4a/dp2a latency
 template <int BL, int L, bool GEN>
 __global__ void __launch_bounds__(256, 3) ks_kernel(const u64 *__restrict__ in, const u32 *__restrict__ src_idx,
                                                   const u32 *__restrict__ ksk_t, u32 *__restrict__ out21,
@@ -290,14 +301,14 @@ __global__ void __launch_bounds__(256, 3) ks_kernel(const u64 *__restrict__ in, 
     const int tid = threadIdx.x;
     const int ty = tid >> 5, tx = tid & 31;  // 8 x 4 cts, 32 x 4 outputs
     const u32 c0 = blockIdx.y * KS_BM, x0 = blockIdx.x * KS_BN;
-    // one accumulator per byte plane of the KSK word: KSK = p0 + p1 2^8 + p2 2^16
-    int acc[KS_PLANES][4][4];
+    // KSK = lo + hi 2^8 (lo its low byte, hi its upper 13 bits): one
+    // accumulator for the low bytes (dp4a over four rows), one for the upper
+    // parts (dp2a over two rows, twice)
+    int acc_lo[4][4], acc_hi[4][4];
 #pragma unroll
-    for (int b = 0; b < KS_PLANES; b++)
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) acc[b][i][j] = 0;
+        for (int j = 0; j < 4; j++) acc_lo[i][j] = acc_hi[i][j] = 0;
 
     const int dct = tid >> 3, dy = tid & 7;  // decomposition role: 32 cts x 8 coefs
     const u32 dct_c = min(c0 + dct, B - 1);
@@ -324,15 +335,19 @@ __global__ void __launch_bounds__(256, 3) ks_kernel(const u64 *__restrict__ in, 
             u32 dv[4];
 #pragma unroll
             for (int i = 0; i < 4; i++) dv[i] = *reinterpret_cast<const u32 *>(&dsm[ty * 4 + i][4 * g]);
+            const uint4 k0 = reinterpret_cast<const uint4 *>(&ksm[g][0][0])[tx];  // low bytes, rows 0-3
+            const uint4 k1 = reinterpret_cast<const uint4 *>(&ksm[g][1][0])[tx];  // upper parts, rows 0, 1
+            const uint4 k2 = reinterpret_cast<const uint4 *>(&ksm[g][2][0])[tx];  // upper parts, rows 2, 3
+            const u32 w0[4] = {k0.x, k0.y, k0.z, k0.w}, w1[4] = {k1.x, k1.y, k1.z, k1.w},
+                      w2[4] = {k2.x, k2.y, k2.z, k2.w};
 #pragma unroll
-            for (int b = 0; b < KS_PLANES; b++) {
-                const uint4 kv = reinterpret_cast<const uint4 *>(&ksm[g][b][0])[tx];
-                const u32 kk[4] = {kv.x, kv.y, kv.z, kv.w};
+            for (int i = 0; i < 4; i++)
 #pragma unroll
-                for (int i = 0; i < 4; i++)
-#pragma unroll
-                    for (int j = 0; j < 4; j++) acc[b][i][j] = dp4a_us(kk[j], dv[i], acc[b][i][j]);
-            }
+                for (int j = 0; j < 4; j++) {
+                    acc_lo[i][j] = dp4a_us(w0[j], dv[i], acc_lo[i][j]);
+                    acc_hi[i][j] = dp2a_us<false>(w1[j], dv[i], acc_hi[i][j]);
+                    acc_hi[i][j] = dp2a_us<true>(w2[j], dv[i], acc_hi[i][j]);
+                }
         }
         __syncthreads();
     }
@@ -340,8 +355,7 @@ __global__ void __launch_bounds__(256, 3) ks_kernel(const u64 *__restrict__ in, 
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-            sum[i][j] = (u32)acc[0][i][j] + ((u32)acc[1][i][j] << 8) + ((u32)acc[2][i][j] << 16);
+        for (int j = 0; j < 4; j++) sum[i][j] = (u32)acc_lo[i][j] + ((u32)acc_hi[i][j] << 8);
     if (part) {
         // 32-bit wrap-around sums are exact mod 2^21 in any order
 #pragma unroll

@@ -14,7 +14,7 @@ constexpr int KS_W = 21;
 constexpr int KS_BN = 128;                    // key-switch output tile
 constexpr int KS_BM = 32;                     // key-switch ciphertext tile
 constexpr int KS_KC = 8;                      // BLWE mask coefficients per K chunk
-constexpr int KS_PLANES = 3;                  // bytes of a 21-bit KSK word (device layout [K/4][plane][xpad])
+constexpr int KS_PLANES = 3;                  // words per 4 KSK rows and output (device layout [K/4][3][xpad])
 constexpr int KS_SPLIT = 16;                  // K slices of the split-K key switch (batches <= KS_BM)
 constexpr int SLAB_WORDS = 8 * 4 * 256;       // one BR step of BSK: 2x2 polys of 2048
 constexpr size_t SLAB_BYTES = SLAB_WORDS * 8; // 64 KiB
