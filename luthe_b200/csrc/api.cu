@@ -356,36 +356,12 @@ extern "C" int luthe_ks_pbs_graph(luthe_ctx *c, const uint64_t *d_in, const uint
     return LUTHE_OK;
 }
 
-extern "C" int luthe_ks_pbs_host(luthe_ctx *c, const uint64_t *h_in, const uint32_t *h_ids, uint64_t *h_out,
-                                 size_t count)
+// The host-buffer path's copies and launches: the inputs in two chunks on the
+// context's copy stream under the key switch, the full waves' outputs back on
+// it while a tail launch runs.  The caller drains both streams.
+static int enqueue_host_ks_pbs(luthe_ctx *c, const uint64_t *h_in, const uint32_t *h_ids, uint64_t *h_out,
+                               size_t count)
 {
-    int r = need_keys(c);
-    if (r) return r;
-    if (count == 0) return LUTHE_OK;
-    if (!h_in || !h_ids || !h_out) return fail(LUTHE_E_PARAM, "null buffer");
-    CUDA_TRY(cudaSetDevice(c->device));
-    for (size_t i = 0; i < count; i++)
-        if (h_ids[i] >= c->nlut) return fail(LUTHE_E_PARAM, "LUT id %u at %zu out of range", h_ids[i], i);
-    if (count > c->hcap) {
-        drop_graphs(c);
-        dfree(c, c->d_hin, c->hcap * (N + 1) * 8);
-        dfree(c, c->d_hout, c->hcap * (N + 1) * 8);
-        dfree(c, c->d_hids, c->hcap * 4);
-        c->d_hin = c->d_hout = nullptr;
-        c->d_hids = nullptr;
-        c->hcap = 0;
-        if ((r = dalloc(c, (void **)&c->d_hin, count * (N + 1) * 8)) ||
-            (r = dalloc(c, (void **)&c->d_hout, count * (N + 1) * 8)) ||
-            (r = dalloc(c, (void **)&c->d_hids, count * 4)))
-            return r;
-        c->hcap = count;
-    }
-    if ((r = ensure_scratch(c, count))) return r;
-    if (!c->copy_stream) {
-        CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming));
-        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
-    }
     cudaStream_t s = 0;
     const uint32_t n = c->p.lwe_dim;
     const size_t row = (size_t)(N + 1);
@@ -419,8 +395,46 @@ extern "C" int luthe_ks_pbs_host(luthe_ctx *c, const uint64_t *h_in, const uint3
     }
     CUDA_TRY(cudaMemcpyAsync(h_out + early * row, c->d_hout + early * row, (count - early) * row * 8,
                              cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
+    return LUTHE_OK;
+}
+
+extern "C" int luthe_ks_pbs_host(luthe_ctx *c, const uint64_t *h_in, const uint32_t *h_ids, uint64_t *h_out,
+                                 size_t count)
+{
+    int r = need_keys(c);
+    if (r) return r;
+    if (count == 0) return LUTHE_OK;
+    if (!h_in || !h_ids || !h_out) return fail(LUTHE_E_PARAM, "null buffer");
+    CUDA_TRY(cudaSetDevice(c->device));
+    for (size_t i = 0; i < count; i++)
+        if (h_ids[i] >= c->nlut) return fail(LUTHE_E_PARAM, "LUT id %u at %zu out of range", h_ids[i], i);
+    if (count > c->hcap) {
+        drop_graphs(c);
+        dfree(c, c->d_hin, c->hcap * (N + 1) * 8);
+        dfree(c, c->d_hout, c->hcap * (N + 1) * 8);
+        dfree(c, c->d_hids, c->hcap * 4);
+        c->d_hin = c->d_hout = nullptr;
+        c->d_hids = nullptr;
+        c->hcap = 0;
+        if ((r = dalloc(c, (void **)&c->d_hin, count * (N + 1) * 8)) ||
+            (r = dalloc(c, (void **)&c->d_hout, count * (N + 1) * 8)) ||
+            (r = dalloc(c, (void **)&c->d_hids, count * 4)))
+            return r;
+        c->hcap = count;
+    }
+    if ((r = ensure_scratch(c, count))) return r;
+    if (!c->copy_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
+    }
+    r = enqueue_host_ks_pbs(c, h_in, h_ids, h_out, count);
+    // both streams are drained before returning, on an error too: no copy
+    // may still write into the caller's buffer afterwards
+    const cudaError_t e0 = cudaStreamSynchronize(0), e1 = cudaStreamSynchronize(c->copy_stream);
+    if (r) return r;
+    if (e0 != cudaSuccess || e1 != cudaSuccess)
+        return fail(LUTHE_E_CUDA, "stream synchronize: %s", cudaGetErrorString(e0 != cudaSuccess ? e0 : e1));
     return luthe_check_device_error(c);
 }
 
