@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(G * 256) ntt_inv_kernel(const u64 *__restrict_
         const size_t src = poly < count ? poly : count - 1;
         u64 x[1][8];
 #pragma unroll
-        for (int p = 0; p < 8; p++) x[0][p] = gl::mul(in[src * N + ntt::eval_index(t, p)], N_INV);
+        for (int p = 0; p < 8; p++) x[0][p] = gl::div2k(in[src * N + ntt::eval_index(t, p)], 11);  // x N^-1 = x 2^-11
         ntt::inverse<1>(x, buf, tws, t, bar);
         if (poly < count) {
 #pragma unroll
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(G * 256) ntt_inv_kernel(const u64 *__restrict_
 
 // negacyclic product of pairs: INTT(NTT(a) * NTT(b))
 template <int G>
-__global__ void __launch_bounds__(G * 256) ntt_mul_kernel(const u64 *__restrict__ a, const u64 *__restrict__ b,
+__global__ void __launch_bounds__(G * 256, 2) ntt_mul_kernel(const u64 *__restrict__ a, const u64 *__restrict__ b,
                                                            u64 *__restrict__ out, const u64 *__restrict__ tw,
                                                            size_t count)
 {
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(G * 256) ntt_mul_kernel(const u64 *__restrict_
         ntt::forward<2>(x, buf, tws, t, bar);
         u64 r[1][8];
 #pragma unroll
-        for (int p = 0; p < 8; p++) r[0][p] = gl::mul(gl::mul(x[0][p], x[1][p]), N_INV);
+        for (int p = 0; p < 8; p++) r[0][p] = gl::div2k(gl::mul(x[0][p], x[1][p]), 11);  // N^-1 = 2^-11: one exact division
         ntt::group_sync(bar);
         ntt::inverse<1>(r, buf, tws + 2048, t, bar);
         if (pr < count) {

@@ -52,7 +52,7 @@ def test_ntt_inverse_roundtrip(engine, count):
     assert np.array_equal(from_dev(d_b, np.uint64), a)
 
 
-@pytest.mark.parametrize("count", [1, 7])
+@pytest.mark.parametrize("count", [1, 7, 1001])  # 1001: more pairs than one wave of CTAs, odd count
 def test_ntt_mul_matches_oracle(engine, count):
     rng = np.random.default_rng(30 + count)
     a, b = rand_p(rng, (count, N)), rand_p(rng, (count, N))
