@@ -76,24 +76,34 @@ def enc_pbs(op, dst, src, gid):
 
 
 class Program:
-    """DOp program builder with a register allocator over the 128-entry file."""
+    """DOp program builder with a register allocator over the 128-entry file.
+
+    Freed registers are reused first in, first out.  The scheduler orders a
+    write after every earlier read of the same register (write-after-read), so
+    handing out the register freed last would make each new value wait for the
+    PBS that read the old one: the MUL program's critical path was 45 PBS
+    levels that way against 14 by its data, the compare's 12 against 5.
+    """
 
     def __init__(self, n_src, n_dst):
         self.words = []
         self.n_src, self.n_dst = n_src, n_dst
-        self.free = list(range(127, -1, -1))
+        self.free = list(range(128))  # least recently freed first
 
     def reg(self):
-        return self.free.pop()
+        return self.free.pop(0)
 
     def pair(self, k=2):
-        """k consecutive registers starting at a multiple of k (many-LUT destination)."""
-        for base in range(0, 128, k):
-            if all(r in self.free for r in range(base, base + k)):
-                for r in range(base, base + k):
-                    self.free.remove(r)
-                return base
-        raise RuntimeError("register file exhausted")
+        """k consecutive registers starting at a multiple of k (many-LUT
+        destination): of the aligned free blocks, the one freed longest ago."""
+        pos = {r: i for i, r in enumerate(self.free)}
+        blocks = [b for b in range(0, 128, k) if all(r in pos for r in range(b, b + k))]
+        if not blocks:
+            raise RuntimeError("register file exhausted")
+        base = min(blocks, key=lambda b: max(pos[r] for r in range(b, b + k)))
+        for r in range(base, base + k):
+            self.free.remove(r)
+        return base
 
     def release(self, *rs):
         for r in rs:

@@ -56,3 +56,40 @@ def test_many_lut_table_layout():
     t = I.LUTS["ManyCarryMsg"]
     for x in range(8):
         assert t[x] == x & 3 and t[8 + x] == x >> 2
+
+
+def _pbs_depth(words, ordered_reuse):
+    """Critical path of a program in PBS levels (ALU DOps take no level), with
+    the serving loop's dependency rules: read-after-write always, and with
+    ordered_reuse also write-after-write and write-after-read, under which a
+    write waits for every earlier reader of the register to finish."""
+    done, reads_done, depth = {}, {}, 0
+    for w in (int(x) for x in words):
+        op, dst, s0, s1 = w >> 26, w & 0x7F, (w >> 7) & 0x7F, (w >> 14) & 0x7F
+        if op >> 4 == 0b10:  # LD / ST
+            srcs, dsts, cost = ([], [dst], 0) if op == I.OPC["LD"] else ([dst], [], 0)
+        elif op >> 4 == 0b11:  # PBS, PBS_MLk: k destinations
+            k = {I.OPC["PBS"]: 1, I.OPC["PBS_ML2"]: 2, I.OPC["PBS_ML4"]: 4, I.OPC["PBS_ML8"]: 8}[op]
+            srcs, dsts, cost = [s0], list(range(dst, dst + k)), 1
+        else:
+            two = op in (I.OPC["ADD"], I.OPC["SUB"], I.OPC["MAC"])
+            srcs, dsts, cost = ([s0, s1] if two else [s0]), [dst], 0
+        start = max([done.get(s, 0) for s in srcs], default=0)
+        if ordered_reuse:
+            start = max([start] + [max(done.get(d, 0), reads_done.get(d, 0)) for d in dsts])
+        end = start + cost
+        for s in srcs:
+            reads_done[s] = max(reads_done.get(s, 0), end)
+        for d in dsts:
+            done[d], reads_done[d] = end, 0
+        depth = max(depth, end)
+    return depth
+
+
+def test_register_reuse_adds_no_pbs_level():
+    """The allocator's register reuse lengthens no program's critical path:
+    with write-after-read and write-after-write ordering the depth equals the
+    data-only depth (ADD 8, compare 5, MUL 14 PBS levels)."""
+    for prog, want in ((I.prog_add(), 8), (I.prog_cmp_gt(0x1234), 5), (I.prog_mul(), 14)):
+        assert _pbs_depth(prog, False) == want
+        assert _pbs_depth(prog, True) == want
