@@ -205,13 +205,16 @@ def max_over_ranks(x, dist, device):
     return float(t.item())
 
 
-def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_per_kind=8, window_us=0, fill=0):
+def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_per_kind=8, window_us=0, fill=0,
+            add="ripple"):
     """Serving loop under Poisson arrivals of 16-bit radix IOps (50 % ADD with
     carry propagation, 30 % scalar compare, 20 % multiply); every result is
     checked by decryption, and with `ob` (an oracle BSK) the first
     `check_per_kind` requests of each kind bit for bit against the oracle's
-    run of the same DOp programs (not timed)."""
+    run of the same DOp programs (not timed).  `add` picks the ADD program:
+    "ripple" (8 PBS in a chain of 8 levels) or "prefix" (24 PBS, 5 levels)."""
     from luthe_b200 import iops as I
+    prog_add = {"ripple": I.prog_add, "prefix": I.prog_add_prefix}[add]
     eng.upload_luts(np.stack([L.lut_build(params, t) for t in I.lut_tables()]))
     rng = np.random.default_rng(seed)
     kinds = rng.choice(3, size=n_req, p=[0.5, 0.3, 0.2])
@@ -221,7 +224,7 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
     for r in range(n_req):
         a, b = int(vals[r, 0]), int(vals[r, 1])
         if kinds[r] == 0:
-            reqs.append([I.prog_add(), 16, 8])
+            reqs.append([prog_add(), 16, 8])
             expect.append((a + b) % 65536)
             blocks += I.to_blocks(a) + I.to_blocks(b)
         elif kinds[r] == 1:
@@ -274,7 +277,7 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
         eq = sum(bool(np.array_equal(outs[r], w)) for r, w in zip(sel, want))
         exact = f"{eq}/{len(sel)} (first {check_per_kind} requests of each kind, MUL included)"
     return {"requests": n_req, "arrival_rate_per_s": rate, "mix": "50% add, 30% scalar cmp, 20% mul (16-bit radix)",
-            "batching_window_us": window_us, "batching_fill": fill or "one wave (2 per SM)",
+            "add_program": add, "batching_window_us": window_us, "batching_fill": fill or "one wave (2 per SM)",
             "bit_exact_vs_oracle": exact,
             "throughput_requests_per_s": n_req / wall, "pbs_per_s": cnt["pbs"] / wall,
             "latency_ms_p50": float(np.percentile(ls, 50)), "latency_ms_p99": float(np.percentile(ls, 99)),
@@ -638,7 +641,7 @@ def main():
     # ---- serving loop (one GPU): Poisson arrivals of radix IOps
     # at 300 req/s offered (above the loop's capacity for this mix: the queue
     # grows) and at 150 req/s (inside it)
-    serve = serve_light = serve_win = serve_light_win = None
+    serve = serve_light = serve_win = serve_light_win = serve_pfx = serve_light_pfx = None
     if world == 1 and not args.no_serving:
         import oracle
         serve_ob = oracle.OracleBsk(keys["bsk"], params.lwe_dim, params.poly_size) if args.cpu_sample > 0 else None
@@ -648,6 +651,9 @@ def main():
         # to 3 ms for more work while another batch is on the GPU
         serve_win = serving(L, eng, params, keys, args.seed + 99, window_us=3000)
         serve_light_win = serving(L, eng, params, keys, args.seed + 98, rate=150.0, window_us=3000)
+        # the same loads with the parallel-prefix ADD (5 PBS levels, 3x its PBS)
+        serve_pfx = serving(L, eng, params, keys, args.seed + 99, ob=serve_ob, add="prefix")
+        serve_light_pfx = serving(L, eng, params, keys, args.seed + 98, rate=150.0, add="prefix")
 
     # ---- CPU baseline (rank 0, one GPU): the CPU restatement on all host cores
     cpu = None
@@ -706,6 +712,8 @@ def main():
             "serving_150": serve_light,
             "serving_window_3ms": serve_win,
             "serving_150_window_3ms": serve_light_win,
+            "serving_prefix_add": serve_pfx,
+            "serving_150_prefix_add": serve_light_pfx,
             "other_configs": other,
             "param_sets": psets,
         }

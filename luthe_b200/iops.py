@@ -11,6 +11,9 @@ fw/ublaze/src/hpu_dop_fmt.h:49-117 (opcodes: include/luthe.h).
 
     ADD      a + b mod 2^16: blockwise ADD, then a carry chain of PBS_ML2
              (message and carry of a block from one blind rotation)
+    ADD (prefix)  the same sum with the carries resolved by a parallel prefix
+             of block carry states: 5 PBS levels instead of 8, 24 PBS
+             instead of 8
     CMP_GT   a > k for a clear 16-bit k: per-block sign PBS, a 3-level tree of
              bivariate combine PBS (MSB block decides), a final PBS to {0, 1}
     MUL      a * b mod 2^16: schoolbook digit products (bivariate PBS on
@@ -45,6 +48,10 @@ LUTS = {
     "ManyCarryMsg": _many(lambda x: x & 3, lambda x: x >> 2),
     "CmpCombine": [(x >> 2) if (x >> 2) != 1 else (x & 3) for x in range(16)],
     "IsTwo": [1 if x == 2 else 0 for x in range(16)],
+    # carry state of a block sum s = a_i + b_i <= 6: 2 generates, 1 propagates, 0 stops
+    "BlockState": [2 if x >= 4 else 1 if x == 3 else 0 for x in range(16)],
+    "BlockState0": [2 if x >= 4 else 0 for x in range(16)],  # no carry into block 0
+    "HalfMsg": [(x >> 1) & 3 for x in range(16)],             # (2 s + 2 c) / 2 mod 4
 }
 for _k in range(4):
     LUTS[f"Cmp{_k}"] = [0 if (x & 3) < _k else 1 if (x & 3) == _k else 2 for x in range(16)]
@@ -157,6 +164,61 @@ def prog_add():
             d = p.reg()
             p.pbs(d, a[i], "MsgOnly")
             p.st(i, d)
+    return p.array()
+
+
+def prog_add_prefix():
+    """a + b mod 2^16 with the carries resolved by a parallel prefix: 5 PBS
+    levels instead of the ripple chain's 8, for 24 PBS instead of 8.
+
+    Level 1 classifies each block sum s_i = a_i + b_i (<= 6) as generate (2),
+    propagate (1) or stop (0) (block 0: generate or stop, no carry comes in);
+    three Sklansky rounds combine the states of blocks 0..i with the compare
+    program's combine LUT (the upper state unless it propagates); the prefix
+    of blocks 0..i-1 is then 0 or 2, and block i's digit is (2 s_i + prefix) / 2
+    mod 4 from one more PBS.
+    """
+    p = Program(2 * BLOCKS, BLOCKS)
+    a = [p.reg() for _ in range(BLOCKS)]
+    b = [p.reg() for _ in range(BLOCKS)]
+    for i in range(BLOCKS):
+        p.ld(a[i], i)
+        p.ld(b[i], BLOCKS + i)
+    for i in range(BLOCKS):
+        p.add(a[i], a[i], b[i])                   # s_i <= 6
+        p.release(b[i])
+    d = p.reg()
+    p.pbs(d, a[0], "MsgOnly")
+    p.st(0, d)
+    p.release(d)
+    pre = []
+    for i in range(BLOCKS - 1):
+        r = p.reg()
+        p.pbs(r, a[i], "BlockState0" if i == 0 else "BlockState")
+        pre.append(r)
+    p.release(a[0])
+    span = 1
+    while span < BLOCKS - 1:                      # pre[i]: state of blocks (i - i mod 2 span) .. i
+        new = list(pre)
+        for i in range(BLOCKS - 1):
+            if (i // span) % 2 == 1:
+                j = (i // span) * span - 1        # last block of the lower half
+                x = p.reg()
+                p.mac(x, pre[i], pre[j], 4)       # hi * 4 + lo <= 10
+                r = p.reg()
+                p.pbs(r, x, "CmpCombine")
+                p.release(x)
+                new[i] = r
+        p.release(*[old for old, nw in zip(pre, new) if old != nw])
+        pre, span = new, 2 * span
+    for i in range(1, BLOCKS):
+        y = p.reg()
+        p.mac(y, a[i], pre[i - 1], 2)             # 2 s_i + (0 or 2) <= 14
+        d = p.reg()
+        p.pbs(d, y, "HalfMsg")
+        p.st(i, d)
+        p.release(y, d, a[i])
+    p.release(*pre)
     return p.array()
 
 

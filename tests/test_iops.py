@@ -15,6 +15,7 @@ def test_add_and_mul_edges(a, b):
     src = I.to_blocks(a) + I.to_blocks(b)
     assert I.from_blocks(I.run_plain(I.prog_add(), src, 8)) == (a + b) % 65536
     assert I.from_blocks(I.run_plain(I.prog_mul(), src, 8)) == (a * b) % 65536
+    assert I.from_blocks(I.run_plain(I.prog_add_prefix(), src, 8)) == (a + b) % 65536
 
 
 @pytest.mark.parametrize("a,k", [(x, y) for x in EDGE for y in EDGE[::2]])
@@ -29,6 +30,7 @@ def test_random_programs():
         src = I.to_blocks(a) + I.to_blocks(b)
         assert I.from_blocks(I.run_plain(I.prog_add(), src, 8)) == (a + b) % 65536
         assert I.from_blocks(I.run_plain(I.prog_mul(), src, 8)) == (a * b) % 65536
+        assert I.from_blocks(I.run_plain(I.prog_add_prefix(), src, 8)) == (a + b) % 65536
         assert I.run_plain(I.prog_cmp_gt(k), I.to_blocks(a), 1) == [int(a > k)]
 
 
@@ -45,7 +47,7 @@ def test_dop_field_layout():
 
 
 def test_programs_fit_the_register_file():
-    for prog in (I.prog_add(), I.prog_cmp_gt(0x1234), I.prog_mul()):
+    for prog in (I.prog_add(), I.prog_cmp_gt(0x1234), I.prog_mul(), I.prog_add_prefix()):
         for w in prog:
             w = int(w)
             assert w & 0x7F < 128
@@ -89,7 +91,20 @@ def _pbs_depth(words, ordered_reuse):
 def test_register_reuse_adds_no_pbs_level():
     """The allocator's register reuse lengthens no program's critical path:
     with write-after-read and write-after-write ordering the depth equals the
-    data-only depth (ADD 8, compare 5, MUL 14 PBS levels)."""
-    for prog, want in ((I.prog_add(), 8), (I.prog_cmp_gt(0x1234), 5), (I.prog_mul(), 14)):
+    data-only depth (ADD 8, compare 5, MUL 14, prefix ADD 5 PBS levels)."""
+    for prog, want in ((I.prog_add(), 8), (I.prog_cmp_gt(0x1234), 5), (I.prog_mul(), 14), (I.prog_add_prefix(), 5)):
         assert _pbs_depth(prog, False) == want
         assert _pbs_depth(prog, True) == want
+
+
+def test_prefix_add_exhaustive_carry_patterns():
+    """Every pattern of per-block carry states: block sums 0..6 in each of the
+    8 blocks would be 7^8 cases, so the 3^8 patterns of stop / propagate /
+    generate (block sums 0, 3, 6) cover every prefix the Sklansky rounds see."""
+    import itertools
+    prog = I.prog_add_prefix()
+    for states in itertools.product((0, 3, 6), repeat=I.BLOCKS):
+        a = [min(s, 3) for s in states]
+        b = [s - x for s, x in zip(states, a)]
+        want = (I.from_blocks(a) + I.from_blocks(b)) % 65536
+        assert I.from_blocks(I.run_plain(prog, a + b, 8)) == want, states
