@@ -563,11 +563,21 @@ extern "C" int luthe_server_step(luthe_server *s, uint32_t *n_completed, uint32_
             }
             r->ready.swap(keep);
         }
+        // Cluster pairs hold two SMs per ciphertext for about 7 ms.  When the
+        // ciphertexts already on the GPU and this batch would need more SMs
+        // than there are, pairs would queue for SMs; the batch then runs one
+        // ciphertext per CTA instead (10.4 ms on one SM: about 40 % more
+        // bootstraps per SM-second).
+        size_t inflight = 0;
+        for (const Lane &o : s->lanes)
+            if (o.busy) inflight += o.ops.size();
+        BrConfig cfg = c->br;
+        if (2 * (inflight + B) > (size_t)c->nsm) cfg.pair_max = 0;
         CUDA_TRY(cudaStreamWaitEvent(ln.stream, s->alu_done, 0));
         CUDA_TRY(cudaMemcpyAsync(ln.d_idx, ln.h_idx, (size_t)s->max_pbs * 3 * 4, cudaMemcpyHostToDevice, ln.stream));
         CUDA_TRY(launch_keyswitch(s->d_pool, c->d_ksk, nullptr, ln.d_l2n, B, n, c->xpad, ln.stream, ln.d_idx, c->p.ks_base_log, c->p.ks_level, c->tie_rule,
                                   ln.d_part));
-        CUDA_TRY(launch_blind_rotate(c->br, c->nsm, ln.d_l2n, c->d_luts, ln.d_idx + 2 * s->max_pbs, c->nlut,
+        CUDA_TRY(launch_blind_rotate(cfg, c->nsm, ln.d_l2n, c->d_luts, ln.d_idx + 2 * s->max_pbs, c->nlut,
                                      c->d_bsk, c->d_tw, s->d_pool, B, n, c->d_err, ln.stream,
                                      ln.d_idx + s->max_pbs, mlk, c->p.pbs_base_log, c->tie_rule));
         CUDA_TRY(cudaEventRecord(ln.done, ln.stream));

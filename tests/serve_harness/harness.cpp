@@ -62,11 +62,14 @@ cudaError_t launch_keyswitch(const uint64_t *in, const uint32_t *, uint32_t *, u
     for (size_t c = 0; c < B; c++) out2N[c * (n + 1)] = (uint32_t)in[(size_t)(src_idx ? src_idx[c] : c) * g_w];
     return cudaSuccess;
 }
-cudaError_t launch_blind_rotate(const BrConfig &, int, const uint32_t *l2n, const uint64_t *luts, const uint32_t *ids,
+// launches seen: batch size and the cluster-pair cut-off the scheduler passed
+static std::vector<std::pair<size_t, int>> g_launch_log;
+cudaError_t launch_blind_rotate(const BrConfig &cfg, int, const uint32_t *l2n, const uint64_t *luts, const uint32_t *ids,
                                 uint32_t, const uint64_t *, const uint64_t *, uint64_t *out, size_t B, uint32_t n,
                                 uint32_t *, cudaStream_t, const uint32_t *dst_idx, uint32_t mlk, uint32_t, uint32_t,
                                 cudaEvent_t, size_t *)
 {
+    g_launch_log.push_back({B, cfg.pair_max});
     for (size_t c = 0; c < B; c++) {
         const uint32_t x = l2n[c * (n + 1)];
         if (x >= 16 / mlk) return cudaErrorInvalidValue;  // payload out of the LUT's range
@@ -91,6 +94,19 @@ extern "C" luthe_ctx *harness_ctx(uint32_t n, const uint64_t *tables, uint32_t n
     return c;
 }
 extern "C" void harness_set_event_lag(int polls) { g_fake_event_lag = polls; }
+extern "C" void harness_set_nsm(luthe_ctx *c, int nsm) { c->nsm = nsm; }
+// copies up to cap logged launches (batch size, pair cut-off), clears the log,
+// returns how many there were
+extern "C" int harness_launch_log(int64_t *batch, int *pair_max, int cap)
+{
+    const int n = (int)luthe::g_launch_log.size();
+    for (int i = 0; i < n && i < cap; i++) {
+        batch[i] = (int64_t)luthe::g_launch_log[i].first;
+        pair_max[i] = luthe::g_launch_log[i].second;
+    }
+    luthe::g_launch_log.clear();
+    return n;
+}
 
 extern "C" void harness_ctx_free(luthe_ctx *c)
 {

@@ -33,6 +33,9 @@ def H():
     lib.luthe_server_set_batching.argtypes = [vp, u32, u32]
     lib.luthe_server_counters.argtypes = [vp] + [ctypes.POINTER(u64)] * 4
     lib.harness_set_event_lag.argtypes = [ctypes.c_int]
+    lib.harness_set_nsm.argtypes = [vp, ctypes.c_int]
+    lib.harness_launch_log.argtypes = [vp, vp, ctypes.c_int]
+    lib.harness_launch_log.restype = ctypes.c_int
     return lib
 
 
@@ -194,3 +197,29 @@ def test_batching_window_holds_partial_batches_and_stays_correct(H):
             H.harness_set_event_lag(0)
         assert [I.from_blocks(o) for o in outs] == expect
     assert launches[10_000_000] < launches[0]
+
+
+def test_loaded_gpu_runs_small_batches_one_per_cta(H):
+    """Cluster pairs take two SMs per ciphertext: a batch whose ciphertexts,
+    with those of the busy lanes, would need more SMs than the device has runs
+    one ciphertext per CTA (pair cut-off 0); an idle device keeps the default
+    cut-off.  Lanes stay busy across steps (events lag), the device has 8 SMs
+    (room for 4 pairs), and the results stay right."""
+    H.harness_set_event_lag(3)
+    try:
+        s = PlainServer(H, 1 << 15)
+        H.harness_set_nsm(s.ctx, 8)
+        H.harness_launch_log(None, None, 0)
+        reqs, expect = _mixed(random.Random(12), 24)
+        outs = run_staggered(s, reqs)
+        batch, pair_max = np.zeros(100000, np.int64), np.zeros(100000, np.int32)
+        n = H.harness_launch_log(batch.ctypes.data, pair_max.ctypes.data, len(batch))
+        s.close()
+    finally:
+        H.harness_set_event_lag(0)
+    assert [I.from_blocks(o) for o in outs] == expect
+    batch, pair_max = batch[:n], pair_max[:n]
+    assert n > 0 and set(pair_max.tolist()) <= {-1, 0}
+    assert np.all(pair_max[2 * batch > 8] == 0)             # alone too big for the pairs
+    assert np.any((pair_max == 0) & (2 * batch <= 8))       # too big with the busy lanes' ciphertexts
+    assert np.any(pair_max == -1)                           # room left: the default cut-off
