@@ -206,15 +206,17 @@ def max_over_ranks(x, dist, device):
 
 
 def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_per_kind=8, window_us=0, fill=0,
-            add="ripple"):
+            programs="fewest_pbs"):
     """Serving loop under Poisson arrivals of 16-bit radix IOps (50 % ADD with
     carry propagation, 30 % scalar compare, 20 % multiply); every result is
     checked by decryption, and with `ob` (an oracle BSK) the first
     `check_per_kind` requests of each kind bit for bit against the oracle's
-    run of the same DOp programs (not timed).  `add` picks the ADD program:
-    "ripple" (8 PBS in a chain of 8 levels) or "prefix" (24 PBS, 5 levels)."""
+    run of the same DOp programs (not timed).  `programs` picks the ADD and
+    MUL programs: "fewest_pbs" (ADD 8 PBS in 8 levels, MUL 101 PBS in 14) or
+    "low_depth" (ADD 24 PBS in 5 levels, MUL 125 PBS in 8)."""
     from luthe_b200 import iops as I
-    prog_add = {"ripple": I.prog_add, "prefix": I.prog_add_prefix}[add]
+    prog_add, prog_mul = {"fewest_pbs": (I.prog_add, I.prog_mul),
+                          "low_depth": (I.prog_add_prefix, I.prog_mul_wallace)}[programs]
     eng.upload_luts(np.stack([L.lut_build(params, t) for t in I.lut_tables()]))
     rng = np.random.default_rng(seed)
     kinds = rng.choice(3, size=n_req, p=[0.5, 0.3, 0.2])
@@ -232,7 +234,7 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
             expect.append(int(a > b))
             blocks += I.to_blocks(a)
         else:
-            reqs.append([I.prog_mul(), 16, 8])
+            reqs.append([prog_mul(), 16, 8])
             expect.append((a * b) % 65536)
             blocks += I.to_blocks(a) + I.to_blocks(b)
     ct = L.encrypt(params, keys["glwe_key"], np.array(blocks, np.uint32), seed + 7)
@@ -277,7 +279,7 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
         eq = sum(bool(np.array_equal(outs[r], w)) for r, w in zip(sel, want))
         exact = f"{eq}/{len(sel)} (first {check_per_kind} requests of each kind, MUL included)"
     return {"requests": n_req, "arrival_rate_per_s": rate, "mix": "50% add, 30% scalar cmp, 20% mul (16-bit radix)",
-            "add_program": add, "batching_window_us": window_us, "batching_fill": fill or "one wave (2 per SM)",
+            "programs": programs, "batching_window_us": window_us, "batching_fill": fill or "one wave (2 per SM)",
             "bit_exact_vs_oracle": exact,
             "throughput_requests_per_s": n_req / wall, "pbs_per_s": cnt["pbs"] / wall,
             "latency_ms_p50": float(np.percentile(ls, 50)), "latency_ms_p99": float(np.percentile(ls, 99)),
@@ -651,9 +653,10 @@ def main():
         # to 3 ms for more work while another batch is on the GPU
         serve_win = serving(L, eng, params, keys, args.seed + 99, window_us=3000)
         serve_light_win = serving(L, eng, params, keys, args.seed + 98, rate=150.0, window_us=3000)
-        # the same loads with the parallel-prefix ADD (5 PBS levels, 3x its PBS)
-        serve_pfx = serving(L, eng, params, keys, args.seed + 99, ob=serve_ob, add="prefix")
-        serve_light_pfx = serving(L, eng, params, keys, args.seed + 98, rate=150.0, add="prefix")
+        # the same loads with the low-depth programs (ADD 5 PBS levels, MUL 8;
+        # more PBS in all)
+        serve_pfx = serving(L, eng, params, keys, args.seed + 99, ob=serve_ob, programs="low_depth")
+        serve_light_pfx = serving(L, eng, params, keys, args.seed + 98, rate=150.0, programs="low_depth")
 
     # ---- CPU baseline (rank 0, one GPU): the CPU restatement on all host cores
     cpu = None
@@ -712,8 +715,8 @@ def main():
             "serving_150": serve_light,
             "serving_window_3ms": serve_win,
             "serving_150_window_3ms": serve_light_win,
-            "serving_prefix_add": serve_pfx,
-            "serving_150_prefix_add": serve_light_pfx,
+            "serving_low_depth": serve_pfx,
+            "serving_150_low_depth": serve_light_pfx,
             "other_configs": other,
             "param_sets": psets,
         }

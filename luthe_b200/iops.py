@@ -19,6 +19,11 @@ fw/ublaze/src/hpu_dop_fmt.h:49-117 (opcodes: include/luthe.h).
     MUL      a * b mod 2^16: schoolbook digit products (bivariate PBS on
              MAC-packed a_i * 4 + b_j, low and high halves), then per-column
              carry-save reduction in groups of up to 5 terms
+    MUL (Wallace)  the same products reduced in parallel rounds over all
+             columns: 8 PBS levels instead of 14, 125 PBS instead of 101
+
+prog_add and prog_mul take the fewest PBS; prog_add_prefix and
+prog_mul_wallace the fewest sequential PBS levels, for more PBS in all.
 """
 import numpy as np
 
@@ -289,6 +294,63 @@ def prog_mul():
             terms.append(m)
         p.st(k, terms[0])
         p.release(terms[0])
+    return p.array()
+
+
+def prog_mul_wallace():
+    """a * b mod 2^16 with the digit products reduced in parallel rounds:
+    8 PBS levels instead of 14, for 125 PBS instead of 101.
+
+    The same digit products as prog_mul (level 1); then every round reduces
+    every column at once: its terms (each <= 3) in groups of up to 5 (sum
+    <= 15), each group to its message (stays) and its carry (to the next
+    column; the top column keeps the message only), a lone term passing
+    through, until every column holds one term.
+    """
+    p = Program(2 * BLOCKS, BLOCKS)
+    a = [p.reg() for _ in range(BLOCKS)]
+    b = [p.reg() for _ in range(BLOCKS)]
+    for i in range(BLOCKS):
+        p.ld(a[i], i)
+        p.ld(b[i], BLOCKS + i)
+    cols = [[] for _ in range(BLOCKS)]
+    for k in range(BLOCKS):
+        for i in range(k + 1):                    # digit products a_i * b_j, i + j = k
+            x = p.reg()
+            p.mac(x, a[i], b[k - i], 4)           # a_i * 4 + b_j
+            lo = p.reg()
+            p.pbs(lo, x, "MultCarryMsgLsb")
+            cols[k].append(lo)
+            if k + 1 < BLOCKS:
+                hi = p.reg()
+                p.pbs(hi, x, "MultCarryMsgMsb")
+                cols[k + 1].append(hi)
+            p.release(x)
+    p.release(*a, *b)
+    while any(len(c) > 1 for c in cols):
+        nxt = [[] for _ in range(BLOCKS)]
+        for k, terms in enumerate(cols):
+            for g in range(0, len(terms), 5):
+                grp = terms[g:g + 5]
+                if len(grp) == 1:
+                    nxt[k].append(grp[0])
+                    continue
+                s = grp[0]
+                for t in grp[1:]:
+                    p.add(s, s, t)
+                    p.release(t)
+                m = p.reg()
+                p.pbs(m, s, "MsgOnly")
+                nxt[k].append(m)
+                if k + 1 < BLOCKS:
+                    c = p.reg()
+                    p.pbs(c, s, "CarryInMsg")
+                    nxt[k + 1].append(c)
+                p.release(s)
+        cols = nxt
+    for k in range(BLOCKS):
+        p.st(k, cols[k][0])
+        p.release(cols[k][0])
     return p.array()
 
 

@@ -16,6 +16,7 @@ def test_add_and_mul_edges(a, b):
     assert I.from_blocks(I.run_plain(I.prog_add(), src, 8)) == (a + b) % 65536
     assert I.from_blocks(I.run_plain(I.prog_mul(), src, 8)) == (a * b) % 65536
     assert I.from_blocks(I.run_plain(I.prog_add_prefix(), src, 8)) == (a + b) % 65536
+    assert I.from_blocks(I.run_plain(I.prog_mul_wallace(), src, 8)) == (a * b) % 65536
 
 
 @pytest.mark.parametrize("a,k", [(x, y) for x in EDGE for y in EDGE[::2]])
@@ -31,6 +32,7 @@ def test_random_programs():
         assert I.from_blocks(I.run_plain(I.prog_add(), src, 8)) == (a + b) % 65536
         assert I.from_blocks(I.run_plain(I.prog_mul(), src, 8)) == (a * b) % 65536
         assert I.from_blocks(I.run_plain(I.prog_add_prefix(), src, 8)) == (a + b) % 65536
+        assert I.from_blocks(I.run_plain(I.prog_mul_wallace(), src, 8)) == (a * b) % 65536
         assert I.run_plain(I.prog_cmp_gt(k), I.to_blocks(a), 1) == [int(a > k)]
 
 
@@ -47,7 +49,7 @@ def test_dop_field_layout():
 
 
 def test_programs_fit_the_register_file():
-    for prog in (I.prog_add(), I.prog_cmp_gt(0x1234), I.prog_mul(), I.prog_add_prefix()):
+    for prog in (I.prog_add(), I.prog_cmp_gt(0x1234), I.prog_mul(), I.prog_add_prefix(), I.prog_mul_wallace()):
         for w in prog:
             w = int(w)
             assert w & 0x7F < 128
@@ -91,8 +93,10 @@ def _pbs_depth(words, ordered_reuse):
 def test_register_reuse_adds_no_pbs_level():
     """The allocator's register reuse lengthens no program's critical path:
     with write-after-read and write-after-write ordering the depth equals the
-    data-only depth (ADD 8, compare 5, MUL 14, prefix ADD 5 PBS levels)."""
-    for prog, want in ((I.prog_add(), 8), (I.prog_cmp_gt(0x1234), 5), (I.prog_mul(), 14), (I.prog_add_prefix(), 5)):
+    data-only depth (ADD 8, compare 5, MUL 14, prefix ADD 5, Wallace MUL 8
+    PBS levels)."""
+    for prog, want in ((I.prog_add(), 8), (I.prog_cmp_gt(0x1234), 5), (I.prog_mul(), 14), (I.prog_add_prefix(), 5),
+                       (I.prog_mul_wallace(), 8)):
         assert _pbs_depth(prog, False) == want
         assert _pbs_depth(prog, True) == want
 
@@ -108,3 +112,10 @@ def test_prefix_add_exhaustive_carry_patterns():
         b = [s - x for s, x in zip(states, a)]
         want = (I.from_blocks(a) + I.from_blocks(b)) % 65536
         assert I.from_blocks(I.run_plain(prog, a + b, 8)) == want, states
+
+
+def test_pbs_counts():
+    """PBS per program: the fewest-PBS forms and the low-depth forms."""
+    count = lambda prog: sum(1 for w in prog if (int(w) >> 26) >> 4 == 0b11)
+    assert [count(I.prog_add()), count(I.prog_cmp_gt(7)), count(I.prog_mul())] == [8, 16, 101]
+    assert [count(I.prog_add_prefix()), count(I.prog_mul_wallace())] == [24, 125]
