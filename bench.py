@@ -212,10 +212,12 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
     checked by decryption, and with `ob` (an oracle BSK) the first
     `check_per_kind` requests of each kind bit for bit against the oracle's
     run of the same DOp programs (not timed).  `programs` picks the ADD and
-    MUL programs: "fewest_pbs" (ADD 8 PBS in 8 levels, MUL 101 PBS in 14) or
-    "low_depth" (ADD 24 PBS in 5 levels, MUL 125 PBS in 8)."""
+    MUL programs: "fewest_pbs" (ADD 8 PBS in 8 levels, MUL 101 PBS in 14),
+    "low_depth" (ADD 24 PBS in 5 levels, MUL 125 PBS in 8) or "adaptive"
+    (per request at submission, by the number of requests in flight:
+    iops.programs_for_load)."""
     from luthe_b200 import iops as I
-    prog_add, prog_mul = {"fewest_pbs": (I.prog_add, I.prog_mul),
+    prog_add, prog_mul = {"fewest_pbs": (I.prog_add, I.prog_mul), "adaptive": (I.prog_add, I.prog_mul),
                           "low_depth": (I.prog_add_prefix, I.prog_mul_wallace)}[programs]
     eng.upload_luts(np.stack([L.lut_build(params, t) for t in I.lut_tables()]))
     rng = np.random.default_rng(seed)
@@ -237,6 +239,7 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
             reqs.append([prog_mul(), 16, 8])
             expect.append((a * b) % 65536)
             blocks += I.to_blocks(a) + I.to_blocks(b)
+    n_low_add, n_low_mul = len(I.prog_add_prefix()), len(I.prog_mul_wallace())
     ct = L.encrypt(params, keys["glwe_key"], np.array(blocks, np.uint32), seed + 7)
     off = 0
     for r in reqs:
@@ -251,6 +254,9 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
     while len(outs) < n_req:
         now = time.perf_counter() - t0
         while sub < n_req and arrivals[sub] <= now:
+            if programs == "adaptive" and kinds[sub] != 1:
+                add_p, mul_p = I.programs_for_load(sub - len(outs))
+                reqs[sub][0] = add_p() if kinds[sub] == 0 else mul_p()
             ids[sub] = srv.submit(*reqs[sub])
             sub += 1
         if sub == len(outs):
@@ -279,7 +285,10 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
         eq = sum(bool(np.array_equal(outs[r], w)) for r, w in zip(sel, want))
         exact = f"{eq}/{len(sel)} (first {check_per_kind} requests of each kind, MUL included)"
     return {"requests": n_req, "arrival_rate_per_s": rate, "mix": "50% add, 30% scalar cmp, 20% mul (16-bit radix)",
-            "programs": programs, "batching_window_us": window_us, "batching_fill": fill or "one wave (2 per SM)",
+            "programs": programs,
+            "low_depth_share": (sum(len(r[0]) in (n_low_add, n_low_mul) for r in reqs) / max(1, int((kinds != 1).sum()))
+                                if programs == "adaptive" else None),
+            "batching_window_us": window_us, "batching_fill": fill or "one wave (2 per SM)",
             "bit_exact_vs_oracle": exact,
             "throughput_requests_per_s": n_req / wall, "pbs_per_s": cnt["pbs"] / wall,
             "latency_ms_p50": float(np.percentile(ls, 50)), "latency_ms_p99": float(np.percentile(ls, 99)),
@@ -643,7 +652,7 @@ def main():
     # ---- serving loop (one GPU): Poisson arrivals of radix IOps
     # at 300 req/s offered (above the loop's capacity for this mix: the queue
     # grows) and at 150 req/s (inside it)
-    serve = serve_light = serve_win = serve_light_win = serve_pfx = serve_light_pfx = None
+    serve = serve_light = serve_win = serve_light_win = serve_pfx = serve_light_pfx = serve_ad = serve_light_ad = None
     if world == 1 and not args.no_serving:
         import oracle
         serve_ob = oracle.OracleBsk(keys["bsk"], params.lwe_dim, params.poly_size) if args.cpu_sample > 0 else None
@@ -657,6 +666,9 @@ def main():
         # more PBS in all)
         serve_pfx = serving(L, eng, params, keys, args.seed + 99, ob=serve_ob, programs="low_depth")
         serve_light_pfx = serving(L, eng, params, keys, args.seed + 98, rate=150.0, programs="low_depth")
+        # and with the programs chosen per request by the load at submission
+        serve_ad = serving(L, eng, params, keys, args.seed + 99, ob=serve_ob, programs="adaptive")
+        serve_light_ad = serving(L, eng, params, keys, args.seed + 98, rate=150.0, programs="adaptive")
 
     # ---- CPU baseline (rank 0, one GPU): the CPU restatement on all host cores
     cpu = None
@@ -717,6 +729,8 @@ def main():
             "serving_150_window_3ms": serve_light_win,
             "serving_low_depth": serve_pfx,
             "serving_150_low_depth": serve_light_pfx,
+            "serving_adaptive": serve_ad,
+            "serving_150_adaptive": serve_light_ad,
             "other_configs": other,
             "param_sets": psets,
         }

@@ -354,6 +354,17 @@ def prog_mul_wallace():
     return p.array()
 
 
+def programs_for_load(in_flight, light=16):
+    """(ADD, MUL) program builders for a request submitted while `in_flight`
+    requests are queued or running: the low-depth forms while the loop is
+    light (fewer sequential PBS, lower latency while the GPU has room), the
+    fewest-PBS forms once it is loaded (the low-depth forms' extra PBS then
+    queue behind each other)."""
+    if in_flight < light:
+        return prog_add_prefix, prog_mul_wallace
+    return prog_add, prog_mul
+
+
 # ------------------------------------------------------ plaintext reference
 
 def run_plain(words, src, n_dst):

@@ -119,3 +119,10 @@ def test_pbs_counts():
     count = lambda prog: sum(1 for w in prog if (int(w) >> 26) >> 4 == 0b11)
     assert [count(I.prog_add()), count(I.prog_cmp_gt(7)), count(I.prog_mul())] == [8, 16, 101]
     assert [count(I.prog_add_prefix()), count(I.prog_mul_wallace())] == [24, 125]
+
+
+def test_programs_for_load():
+    assert I.programs_for_load(0) == (I.prog_add_prefix, I.prog_mul_wallace)
+    assert I.programs_for_load(15) == (I.prog_add_prefix, I.prog_mul_wallace)
+    assert I.programs_for_load(16) == (I.prog_add, I.prog_mul)
+    assert I.programs_for_load(3, light=2) == (I.prog_add, I.prog_mul)
