@@ -15,7 +15,7 @@ fw/ublaze/src/hpu_dop_fmt.h:49-117 (opcodes: include/luthe.h).
              of block carry states: 5 PBS levels instead of 8, 24 PBS
              instead of 8
     CMP_GT   a > k for a clear 16-bit k: per-block sign PBS, a 3-level tree of
-             bivariate combine PBS (MSB block decides), a final PBS to {0, 1}
+             bivariate combine PBS (MSB block decides) whose root maps to {0, 1}
     MUL      a * b mod 2^16: schoolbook digit products (bivariate PBS on
              MAC-packed a_i * 4 + b_j, low and high halves), then per-column
              carry-save reduction in groups of up to 5 terms
@@ -53,6 +53,8 @@ LUTS = {
     "ManyCarryMsg": _many(lambda x: x & 3, lambda x: x >> 2),
     "CmpCombine": [(x >> 2) if (x >> 2) != 1 else (x & 3) for x in range(16)],
     "IsTwo": [1 if x == 2 else 0 for x in range(16)],
+    # the compare's last combine and the final "greater" test in one table
+    "CmpCombineIsTwo": [1 if ((x >> 2) if (x >> 2) != 1 else (x & 3)) == 2 else 0 for x in range(16)],
     # carry state of a block sum s = a_i + b_i <= 6: 2 generates, 1 propagates, 0 stops
     "BlockState": [2 if x >= 4 else 1 if x == 3 else 0 for x in range(16)],
     "BlockState0": [2 if x >= 4 else 0 for x in range(16)],  # no carry into block 0
@@ -94,7 +96,8 @@ class Program:
     write after every earlier read of the same register (write-after-read), so
     handing out the register freed last would make each new value wait for the
     PBS that read the old one: the MUL program's critical path was 45 PBS
-    levels that way against 14 by its data, the compare's 12 against 5.
+    levels that way against 14 by its data, the compare's 12 against 5 (4
+    since its root combine and final test share one PBS).
     """
 
     def __init__(self, n_src, n_dst):
@@ -241,17 +244,16 @@ def prog_cmp_gt(k):
         p.release(a[i])
     while len(cmp) > 1:                           # cmp[i]: block i, higher index = more significant
         nxt = []
+        last = len(cmp) == 2                      # the root: combine and test "greater" at once
         for lo, hi in zip(cmp[0::2], cmp[1::2]):
             x = p.reg()
             p.mac(x, hi, lo, 4)                   # hi * 4 + lo <= 10
             d = p.reg()
-            p.pbs(d, x, "CmpCombine")
+            p.pbs(d, x, "CmpCombineIsTwo" if last else "CmpCombine")
             p.release(x, hi, lo)
             nxt.append(d)
         cmp = nxt
-    d = p.reg()
-    p.pbs(d, cmp[0], "IsTwo")
-    p.st(0, d)
+    p.st(0, cmp[0])
     return p.array()
 
 

@@ -107,7 +107,7 @@ def test_serving_mix_equals_alone(engine, params, keys, iop_luts):
         assert (I.from_blocks(dec) if nd == 8 else dec[0]) == want
     for m, s in zip(mixed[:3], alone):
         assert np.array_equal(m, s)
-    assert counters["pbs"] == 3 * (8 + 16 + 101) + 8 + 16 + 101
+    assert counters["pbs"] == 3 * (8 + 15 + 101) + 8 + 15 + 101
 
 
 def test_serving_admission_is_bounded_by_the_pool(engine, params, keys, iop_luts):

@@ -93,9 +93,9 @@ def _pbs_depth(words, ordered_reuse):
 def test_register_reuse_adds_no_pbs_level():
     """The allocator's register reuse lengthens no program's critical path:
     with write-after-read and write-after-write ordering the depth equals the
-    data-only depth (ADD 8, compare 5, MUL 14, prefix ADD 5, Wallace MUL 8
+    data-only depth (ADD 8, compare 4, MUL 14, prefix ADD 5, Wallace MUL 8
     PBS levels)."""
-    for prog, want in ((I.prog_add(), 8), (I.prog_cmp_gt(0x1234), 5), (I.prog_mul(), 14), (I.prog_add_prefix(), 5),
+    for prog, want in ((I.prog_add(), 8), (I.prog_cmp_gt(0x1234), 4), (I.prog_mul(), 14), (I.prog_add_prefix(), 5),
                        (I.prog_mul_wallace(), 8)):
         assert _pbs_depth(prog, False) == want
         assert _pbs_depth(prog, True) == want
@@ -117,7 +117,7 @@ def test_prefix_add_exhaustive_carry_patterns():
 def test_pbs_counts():
     """PBS per program: the fewest-PBS forms and the low-depth forms."""
     count = lambda prog: sum(1 for w in prog if (int(w) >> 26) >> 4 == 0b11)
-    assert [count(I.prog_add()), count(I.prog_cmp_gt(7)), count(I.prog_mul())] == [8, 16, 101]
+    assert [count(I.prog_add()), count(I.prog_cmp_gt(7)), count(I.prog_mul())] == [8, 15, 101]
     assert [count(I.prog_add_prefix()), count(I.prog_mul_wallace())] == [24, 125]
 
 
@@ -126,3 +126,15 @@ def test_programs_for_load():
     assert I.programs_for_load(15) == (I.prog_add_prefix, I.prog_mul_wallace)
     assert I.programs_for_load(16) == (I.prog_add, I.prog_mul)
     assert I.programs_for_load(3, light=2) == (I.prog_add, I.prog_mul)
+
+
+def test_compare_exhaustive_on_block_patterns():
+    """a > k for every pair of 8-block values drawn from digits {0, 2, 3}:
+    each block is less, equal or greater in every position."""
+    import itertools
+    vals = [I.from_blocks(ds) for ds in itertools.product((0, 2, 3), repeat=4)]
+    vals = [v | (v << 8) for v in vals] + [v << 8 for v in vals]
+    for k in vals[::7]:
+        prog = I.prog_cmp_gt(k)
+        for a in vals:
+            assert I.run_plain(prog, I.to_blocks(a), 1) == [int(a > k)], (a, k)
