@@ -211,14 +211,14 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
     carry propagation, 30 % scalar compare, 20 % multiply); every result is
     checked by decryption, and with `ob` (an oracle BSK) the first
     `check_per_kind` requests of each kind bit for bit against the oracle's
-    run of the same DOp programs (not timed).  `programs` picks the ADD and
-    MUL programs: "fewest_pbs" (ADD 8 PBS in 8 levels, MUL 101 PBS in 14),
-    "low_depth" (ADD 24 PBS in 5 levels, MUL 125 PBS in 8) or "adaptive"
-    (per request at submission, by the number of requests in flight:
+    run of the same DOp programs (not timed).  `programs` picks the ADD
+    program (MUL has one form, 101 PBS in 8 levels): "fewest_pbs" (ADD 8 PBS
+    in 8 levels), "low_depth" (ADD 24 PBS in 5 levels) or "adaptive" (per
+    request at submission, by the number of requests in flight:
     iops.programs_for_load)."""
     from luthe_b200 import iops as I
     prog_add, prog_mul = {"fewest_pbs": (I.prog_add, I.prog_mul), "adaptive": (I.prog_add, I.prog_mul),
-                          "low_depth": (I.prog_add_prefix, I.prog_mul_wallace)}[programs]
+                          "low_depth": (I.prog_add_prefix, I.prog_mul)}[programs]
     eng.upload_luts(np.stack([L.lut_build(params, t) for t in I.lut_tables()]))
     rng = np.random.default_rng(seed)
     kinds = rng.choice(3, size=n_req, p=[0.5, 0.3, 0.2])
@@ -239,7 +239,7 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
             reqs.append([prog_mul(), 16, 8])
             expect.append((a * b) % 65536)
             blocks += I.to_blocks(a) + I.to_blocks(b)
-    n_low_add, n_low_mul = len(I.prog_add_prefix()), len(I.prog_mul_wallace())
+    n_low_add = len(I.prog_add_prefix())
     ct = L.encrypt(params, keys["glwe_key"], np.array(blocks, np.uint32), seed + 7)
     off = 0
     for r in reqs:
@@ -254,9 +254,8 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
     while len(outs) < n_req:
         now = time.perf_counter() - t0
         while sub < n_req and arrivals[sub] <= now:
-            if programs == "adaptive" and kinds[sub] != 1:
-                add_p, mul_p = I.programs_for_load(sub - len(outs))
-                reqs[sub][0] = add_p() if kinds[sub] == 0 else mul_p()
+            if programs == "adaptive" and kinds[sub] == 0:
+                reqs[sub][0] = I.programs_for_load(sub - len(outs))[0]()
             ids[sub] = srv.submit(*reqs[sub])
             sub += 1
         if sub == len(outs):
@@ -286,7 +285,7 @@ def serving(L, eng, params, keys, seed, n_req=400, rate=300.0, ob=None, check_pe
         exact = f"{eq}/{len(sel)} (first {check_per_kind} requests of each kind, MUL included)"
     return {"requests": n_req, "arrival_rate_per_s": rate, "mix": "50% add, 30% scalar cmp, 20% mul (16-bit radix)",
             "programs": programs,
-            "low_depth_share": (sum(len(r[0]) in (n_low_add, n_low_mul) for r in reqs) / max(1, int((kinds != 1).sum()))
+            "low_depth_share": (sum(len(r[0]) == n_low_add for r in reqs) / max(1, int((kinds == 0).sum()))
                                 if programs == "adaptive" else None),
             "batching_window_us": window_us, "batching_fill": fill or "one wave (2 per SM)",
             "bit_exact_vs_oracle": exact,
@@ -662,8 +661,8 @@ def main():
         # to 3 ms for more work while another batch is on the GPU
         serve_win = serving(L, eng, params, keys, args.seed + 99, window_us=3000)
         serve_light_win = serving(L, eng, params, keys, args.seed + 98, rate=150.0, window_us=3000)
-        # the same loads with the low-depth programs (ADD 5 PBS levels, MUL 8;
-        # more PBS in all)
+        # the same loads with the prefix ADD (5 PBS levels instead of 8, 24 PBS
+        # instead of 8)
         serve_pfx = serving(L, eng, params, keys, args.seed + 99, ob=serve_ob, programs="low_depth")
         serve_light_pfx = serving(L, eng, params, keys, args.seed + 98, rate=150.0, programs="low_depth")
         # and with the programs chosen per request by the load at submission

@@ -18,12 +18,11 @@ fw/ublaze/src/hpu_dop_fmt.h:49-117 (opcodes: include/luthe.h).
              bivariate combine PBS (MSB block decides) whose root maps to {0, 1}
     MUL      a * b mod 2^16: schoolbook digit products (bivariate PBS on
              MAC-packed a_i * 4 + b_j, low and high halves), then per-column
-             carry-save reduction in groups of up to 5 terms
-    MUL (Wallace)  the same products reduced in parallel rounds over all
-             columns: 8 PBS levels instead of 14, 125 PBS instead of 101
+             carry-save reduction in groups of up to 5 terms, earliest-ready
+             terms first (101 PBS, 8 levels)
 
-prog_add and prog_mul take the fewest PBS; prog_add_prefix and
-prog_mul_wallace the fewest sequential PBS levels, for more PBS in all.
+prog_add takes the fewest PBS, prog_add_prefix the fewest sequential PBS
+levels; programs_for_load picks between them by load.
 """
 import numpy as np
 
@@ -258,56 +257,17 @@ def prog_cmp_gt(k):
 
 
 def prog_mul():
-    """a (src 0..7) * b (src 8..15) -> dst blocks 0..7, mod 2^16."""
-    p = Program(2 * BLOCKS, BLOCKS)
-    a = [p.reg() for _ in range(BLOCKS)]
-    b = [p.reg() for _ in range(BLOCKS)]
-    for i in range(BLOCKS):
-        p.ld(a[i], i)
-        p.ld(b[i], BLOCKS + i)
-    cols = [[] for _ in range(BLOCKS)]
-    for k in range(BLOCKS):
-        for i in range(k + 1):                    # digit products a_i * b_j, i + j = k
-            j = k - i
-            x = p.reg()
-            p.mac(x, a[i], b[j], 4)               # a_i * 4 + b_j
-            lo = p.reg()
-            p.pbs(lo, x, "MultCarryMsgLsb")
-            cols[k].append(lo)
-            if k + 1 < BLOCKS:
-                hi = p.reg()
-                p.pbs(hi, x, "MultCarryMsgMsb")
-                cols[k + 1].append(hi)
-            p.release(x)
-        terms = cols[k]
-        while len(terms) > 1:                     # carry-save: <= 5 terms of <= 3 sum to <= 15
-            grp, terms = terms[:5], terms[5:]
-            s = grp[0]
-            for t in grp[1:]:
-                p.add(s, s, t)
-                p.release(t)
-            m = p.reg()
-            p.pbs(m, s, "MsgOnly")
-            if k + 1 < BLOCKS:
-                c = p.reg()
-                p.pbs(c, s, "CarryInMsg")
-                cols[k + 1].append(c)
-            p.release(s)
-            terms.append(m)
-        p.st(k, terms[0])
-        p.release(terms[0])
-    return p.array()
+    """a (src 0..7) * b (src 8..15) -> dst blocks 0..7, mod 2^16: 101 PBS in 8
+    levels.
 
-
-def prog_mul_wallace():
-    """a * b mod 2^16 with the digit products reduced in parallel rounds:
-    8 PBS levels instead of 14, for 125 PBS instead of 101.
-
-    The same digit products as prog_mul (level 1); then every round reduces
-    every column at once: its terms (each <= 3) in groups of up to 5 (sum
-    <= 15), each group to its message (stays) and its carry (to the next
-    column; the top column keeps the message only), a lone term passing
-    through, until every column holds one term.
+    Digit products a_i * b_j (i + j = k) as bivariate PBS on the MAC-packed
+    a_i * 4 + b_j: the low half into column k, the high half into column k+1
+    (level 1).  Each column is then reduced in groups of up to 5 terms (each
+    <= 3, sum <= 15) to a message (stays) and a carry (to the next column; the
+    top column keeps the message only), always grouping the terms that are
+    ready earliest: carries arrive from the column below at later levels, and
+    grouping in arrival order instead of readiness gave 14 levels for the same
+    PBS count.
     """
     p = Program(2 * BLOCKS, BLOCKS)
     a = [p.reg() for _ in range(BLOCKS)]
@@ -315,56 +275,50 @@ def prog_mul_wallace():
     for i in range(BLOCKS):
         p.ld(a[i], i)
         p.ld(b[i], BLOCKS + i)
-    cols = [[] for _ in range(BLOCKS)]
+    cols = [[] for _ in range(BLOCKS)]            # (PBS level at which it is ready, register)
     for k in range(BLOCKS):
         for i in range(k + 1):                    # digit products a_i * b_j, i + j = k
             x = p.reg()
             p.mac(x, a[i], b[k - i], 4)           # a_i * 4 + b_j
             lo = p.reg()
             p.pbs(lo, x, "MultCarryMsgLsb")
-            cols[k].append(lo)
+            cols[k].append((1, lo))
             if k + 1 < BLOCKS:
                 hi = p.reg()
                 p.pbs(hi, x, "MultCarryMsgMsb")
-                cols[k + 1].append(hi)
+                cols[k + 1].append((1, hi))
             p.release(x)
     p.release(*a, *b)
-    while any(len(c) > 1 for c in cols):
-        nxt = [[] for _ in range(BLOCKS)]
-        for k, terms in enumerate(cols):
-            for g in range(0, len(terms), 5):
-                grp = terms[g:g + 5]
-                if len(grp) == 1:
-                    nxt[k].append(grp[0])
-                    continue
-                s = grp[0]
-                for t in grp[1:]:
-                    p.add(s, s, t)
-                    p.release(t)
-                m = p.reg()
-                p.pbs(m, s, "MsgOnly")
-                nxt[k].append(m)
-                if k + 1 < BLOCKS:
-                    c = p.reg()
-                    p.pbs(c, s, "CarryInMsg")
-                    nxt[k + 1].append(c)
-                p.release(s)
-        cols = nxt
     for k in range(BLOCKS):
-        p.st(k, cols[k][0])
-        p.release(cols[k][0])
+        terms = cols[k]
+        while len(terms) > 1:
+            terms.sort()
+            grp, terms = terms[:5], terms[5:]
+            level = max(lv for lv, _ in grp) + 1
+            s = grp[0][1]
+            for _, t in grp[1:]:
+                p.add(s, s, t)
+                p.release(t)
+            m = p.reg()
+            p.pbs(m, s, "MsgOnly")
+            terms.append((level, m))
+            if k + 1 < BLOCKS:
+                c = p.reg()
+                p.pbs(c, s, "CarryInMsg")
+                cols[k + 1].append((level, c))
+            p.release(s)
+        p.st(k, terms[0][1])
+        p.release(terms[0][1])
     return p.array()
 
 
 def programs_for_load(in_flight, light=16):
     """(ADD, MUL) program builders for a request submitted while `in_flight`
-    requests are queued or running: the low-depth forms while the loop is
-    light (fewer sequential PBS, lower latency while the GPU has room), the
-    fewest-PBS forms once it is loaded (the low-depth forms' extra PBS then
-    queue behind each other)."""
-    if in_flight < light:
-        return prog_add_prefix, prog_mul_wallace
-    return prog_add, prog_mul
+    requests are queued or running: the prefix ADD while the loop is light
+    (fewer sequential PBS, lower latency while the GPU has room), the ripple
+    ADD once it is loaded (the prefix form's extra PBS then queue behind each
+    other).  MUL has one form: its fewest-PBS program is also its shallowest."""
+    return (prog_add_prefix if in_flight < light else prog_add), prog_mul
 
 
 # ------------------------------------------------------ plaintext reference

@@ -16,7 +16,6 @@ def test_add_and_mul_edges(a, b):
     assert I.from_blocks(I.run_plain(I.prog_add(), src, 8)) == (a + b) % 65536
     assert I.from_blocks(I.run_plain(I.prog_mul(), src, 8)) == (a * b) % 65536
     assert I.from_blocks(I.run_plain(I.prog_add_prefix(), src, 8)) == (a + b) % 65536
-    assert I.from_blocks(I.run_plain(I.prog_mul_wallace(), src, 8)) == (a * b) % 65536
 
 
 @pytest.mark.parametrize("a,k", [(x, y) for x in EDGE for y in EDGE[::2]])
@@ -32,7 +31,6 @@ def test_random_programs():
         assert I.from_blocks(I.run_plain(I.prog_add(), src, 8)) == (a + b) % 65536
         assert I.from_blocks(I.run_plain(I.prog_mul(), src, 8)) == (a * b) % 65536
         assert I.from_blocks(I.run_plain(I.prog_add_prefix(), src, 8)) == (a + b) % 65536
-        assert I.from_blocks(I.run_plain(I.prog_mul_wallace(), src, 8)) == (a * b) % 65536
         assert I.run_plain(I.prog_cmp_gt(k), I.to_blocks(a), 1) == [int(a > k)]
 
 
@@ -49,7 +47,7 @@ def test_dop_field_layout():
 
 
 def test_programs_fit_the_register_file():
-    for prog in (I.prog_add(), I.prog_cmp_gt(0x1234), I.prog_mul(), I.prog_add_prefix(), I.prog_mul_wallace()):
+    for prog in (I.prog_add(), I.prog_cmp_gt(0x1234), I.prog_mul(), I.prog_add_prefix()):
         for w in prog:
             w = int(w)
             assert w & 0x7F < 128
@@ -93,10 +91,8 @@ def _pbs_depth(words, ordered_reuse):
 def test_register_reuse_adds_no_pbs_level():
     """The allocator's register reuse lengthens no program's critical path:
     with write-after-read and write-after-write ordering the depth equals the
-    data-only depth (ADD 8, compare 4, MUL 14, prefix ADD 5, Wallace MUL 8
-    PBS levels)."""
-    for prog, want in ((I.prog_add(), 8), (I.prog_cmp_gt(0x1234), 4), (I.prog_mul(), 14), (I.prog_add_prefix(), 5),
-                       (I.prog_mul_wallace(), 8)):
+    data-only depth (ADD 8, compare 4, MUL 8, prefix ADD 5 PBS levels)."""
+    for prog, want in ((I.prog_add(), 8), (I.prog_cmp_gt(0x1234), 4), (I.prog_mul(), 8), (I.prog_add_prefix(), 5)):
         assert _pbs_depth(prog, False) == want
         assert _pbs_depth(prog, True) == want
 
@@ -115,15 +111,15 @@ def test_prefix_add_exhaustive_carry_patterns():
 
 
 def test_pbs_counts():
-    """PBS per program: the fewest-PBS forms and the low-depth forms."""
+    """PBS per program: the fewest-PBS forms and the prefix ADD."""
     count = lambda prog: sum(1 for w in prog if (int(w) >> 26) >> 4 == 0b11)
     assert [count(I.prog_add()), count(I.prog_cmp_gt(7)), count(I.prog_mul())] == [8, 15, 101]
-    assert [count(I.prog_add_prefix()), count(I.prog_mul_wallace())] == [24, 125]
+    assert count(I.prog_add_prefix()) == 24
 
 
 def test_programs_for_load():
-    assert I.programs_for_load(0) == (I.prog_add_prefix, I.prog_mul_wallace)
-    assert I.programs_for_load(15) == (I.prog_add_prefix, I.prog_mul_wallace)
+    assert I.programs_for_load(0) == (I.prog_add_prefix, I.prog_mul)
+    assert I.programs_for_load(15) == (I.prog_add_prefix, I.prog_mul)
     assert I.programs_for_load(16) == (I.prog_add, I.prog_mul)
     assert I.programs_for_load(3, light=2) == (I.prog_add, I.prog_mul)
 
