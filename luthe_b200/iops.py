@@ -94,9 +94,8 @@ class Program:
     Freed registers are reused first in, first out.  The scheduler orders a
     write after every earlier read of the same register (write-after-read), so
     handing out the register freed last would make each new value wait for the
-    PBS that read the old one: the MUL program's critical path was 45 PBS
-    levels that way against 14 by its data, the compare's 12 against 5 (4
-    since its root combine and final test share one PBS).
+    PBS that read the old one: that way an earlier MUL program, 14 PBS levels
+    deep by its data, took 45, and the compare 12 instead of 5.
     """
 
     def __init__(self, n_src, n_dst):
